@@ -1,0 +1,701 @@
+// api.cu -- the C ABI (include/fmm_b200.h): contexts, fmm!, direct!, parity
+// exports and single-operator entry points.
+//
+// fmm_solve follows the reference driver (src/fmm.jl:807-1176): trees for the
+// targets and the sources, interaction lists, the influence estimate for the
+// relative error methods, then nearfield -> upward -> horizontal -> downward
+// passes and the unsort of the target buffer.  All stages run on one CUDA
+// stream; the tree and list builders synchronise with the host once per level.
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+#include "context.cuh"
+
+using namespace fmmb;
+
+namespace {
+
+struct Workspace {
+  DevTree tree[2];  // [0] target role, [1] source role (aliased when shared)
+  DevLists lists;
+  DevBuf<double> acc13;  // target buffer rows 4..16, sorted order
+  bool shared = false;
+  DevTree& target() { return shared ? tree[1] : tree[0]; }
+  DevTree& source() { return tree[1]; }
+};
+
+__global__ void k_unsort(const double* __restrict__ acc13, const int* __restrict__ sort_index,
+                         const double4* __restrict__ pos, int64_t n, double* __restrict__ out16) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t o = sort_index ? sort_index[i] : i;
+    double4 p = pos[i];
+    double* d = out16 + 16 * o;
+    d[0] = p.x;
+    d[1] = p.y;
+    d[2] = p.z;
+    const double* a = acc13 + 13 * i;
+#pragma unroll
+    for (int k = 0; k < 13; ++k) d[3 + k] = a[k];
+  }
+}
+
+int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); }
+
+}  // namespace
+
+struct fmm_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool timing = false;
+  size_t budget = 0;
+  std::string err;
+  Workspace main, est;
+  Scratch sc;
+  DevTables tables;
+  DevBuf<double> stage_s, stage_t, out16, est_out16;
+  DevBuf<int> stats;
+  bool have_solve = false;
+  int last_p = 0;
+  int last_kind = 1;
+};
+
+namespace {
+
+int fail(fmm_ctx* c, const Error& e) {
+  if (c) c->err = e.msg;
+  return e.code;
+}
+
+struct SolveIn {
+  const double* src;  // device, body-major d*n_s
+  int d;
+  int kind;
+  int64_t n_s;
+  const double* tpos;  // device, stride (nullptr: the sources are the targets)
+  int64_t t_stride;
+  int64_t n_t;
+};
+
+size_t footprint(const SolveIn& in, const fmm_options& o) {
+  int64_t nt = in.tpos ? in.n_t : in.n_s;
+  int64_t ls = std::max(1, o.leaf_size_source);
+  int64_t nbr = 2 * (nt + in.n_s) / ls + 1024;
+  size_t exp = (size_t)nbr * 4 * nh(o.expansion_order) * 8 * 2;
+  size_t bodies = (size_t)(nt + in.n_s) * (32 + 32 + 8) + (size_t)nt * (13 + 16) * 8;
+  size_t lists = (size_t)nbr * (256 + 64) * 8;
+  size_t scratch = (size_t)(nt + in.n_s) * 48;
+  return exp + bodies + lists + scratch;
+}
+
+// one fmm! evaluation into out16 (device, original target order)
+void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, double* out16, fmm_result* res,
+             bool is_estimate) {
+  cudaStream_t st = c->stream;
+  const int p = o.expansion_order;
+  const bool lh = in.kind == FMM_POINT_VORTEX;
+  const int64_t ls_s = o.leaf_size_source;
+  const int64_t ls_t = o.leaf_size_target > 0 ? o.leaf_size_target : ls_s;
+  const bool ps = o.scalar_potential != 0, gs = o.gradient != 0, hs = o.hessian != 0;
+  cudaEvent_t ev[8] = {};
+  const bool timing = c->timing && !is_estimate && res;
+  if (timing)
+    for (auto& e : ev) FMM_CUDA_TRY(cudaEventCreate(&e));
+  auto mark = [&](int k) {
+    if (timing) FMM_CUDA_TRY(cudaEventRecord(ev[k], st));
+  };
+  mark(0);
+  // ---- trees (src/tree.jl:3-122)
+  DevTree& S = W.tree[1];
+  unpack_bodies(S, in.src, in.n_s, in.d, in.kind, true, st);
+  build_tree(S, c->sc, st, ls_s, o.list_method, o.shrink_recenter != 0);
+  W.shared = (in.tpos == nullptr) && (ls_t == ls_s);
+  if (!W.shared) {
+    DevTree& T = W.tree[0];
+    const double* tp = in.tpos ? in.tpos : in.src;
+    int64_t stride = in.tpos ? in.t_stride : in.d;
+    int64_t nt = in.tpos ? in.n_t : in.n_s;
+    unpack_bodies(T, tp, nt, stride, 0, false, st);
+    build_tree(T, c->sc, st, ls_t, o.list_method, o.shrink_recenter != 0);
+  }
+  DevTree& T = W.target();
+  mark(1);
+  // ---- interaction lists (src/interaction_list.jl:3-19, 183-213)
+  build_lists(W.lists, T, S, c->sc, st, ls_s, o.multipole_acceptance, o.farfield != 0, o.nearfield != 0,
+              o.self_induced != 0, o.list_method);
+  mark(2);
+  // ---- relative error methods: influence estimate (src/fmm.jl:1193-1276)
+  FMM_CUDA_TRY(cudaMemsetAsync(T.max_influence.ptr, 0, T.n_branches * sizeof(double), st));
+  if (o.error_method == FMM_POWER_RELATIVE_GRADIENT || o.error_method == FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT) {
+    fmm_options e = o;
+    e.leaf_size_source = 5;
+    e.leaf_size_target = 5;
+    e.expansion_order = 3;
+    e.multipole_acceptance = 0.6;
+    e.error_method = FMM_ERROR_NONE;
+    e.shrink_recenter = 1;
+    e.list_method = FMM_LIST_SELF_TUNING_TREE_STOP;
+    e.farfield = e.nearfield = e.self_induced = 1;
+    e.upward_pass = e.horizontal_pass = e.downward_pass = 1;
+    e.scalar_potential = 1;
+    e.gradient = 1;
+    e.hessian = 0;
+    e.precision = FMM_PRECISION_F64;
+    int64_t nt = in.tpos ? in.n_t : in.n_s;
+    c->est_out16.grow(16 * (size_t)nt);
+    run_fmm(c, c->est, in, e, c->est_out16.ptr, nullptr, true);
+    branch_max_influence(T, c->est_out16.ptr, st);
+  }
+  mark(3);
+  // ---- evaluation passes (src/fmm.jl:1028-1089)
+  const int64_t NH4 = 4 * nh(p);
+  upload_tables(c->tables, p, st);
+  S.multipole.grow(NH4 * S.n_branches);
+  T.local.grow(NH4 * T.n_branches);
+  FMM_CUDA_TRY(cudaMemsetAsync(S.multipole.ptr, 0, NH4 * S.n_branches * sizeof(double), st));
+  FMM_CUDA_TRY(cudaMemsetAsync(T.local.ptr, 0, NH4 * T.n_branches * sizeof(double), st));
+  W.acc13.grow(13 * (size_t)T.n_bodies);
+  FMM_CUDA_TRY(cudaMemsetAsync(W.acc13.ptr, 0, 13 * T.n_bodies * sizeof(double), st));
+  c->stats.grow(8);
+  FMM_CUDA_TRY(cudaMemsetAsync(c->stats.ptr, 0, 8 * sizeof(int), st));
+  launch_p2p(T, S, W.lists, W.acc13.ptr, in.kind, ps, gs, hs, o.precision, st);
+  mark(4);
+  if (o.upward_pass) {
+    launch_p2m(S, p, in.kind, c->tables, st);
+    launch_m2m(S, p, lh, c->tables, st);
+  }
+  mark(5);
+  if (o.horizontal_pass)
+    launch_m2l(T, S, W.lists, p, lh, o.error_method, o.error_tolerance, o.bonus_expansion, nullptr, c->stats.ptr,
+               c->tables, st);
+  mark(6);
+  if (o.downward_pass) {
+    launch_l2l(T, p, lh, c->tables, st);
+    launch_l2p(T, p, lh, ps, gs, hs, W.acc13.ptr, st);
+  }
+  // ---- unsort into the caller's order (buffer_to_target!, src/compatibility.jl:324-338)
+  k_unsort<<<grid_for(T.n_bodies), 256, 0, st>>>(W.acc13.ptr, T.sort_index.ptr, T.pos.ptr, T.n_bodies, out16);
+  FMM_CUDA_TRY(cudaGetLastError());
+  mark(7);
+  if (res) {
+    int h[4] = {0, 0, 0, 0};
+    FMM_CUDA_TRY(cudaMemcpyAsync(h, c->stats.ptr, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    FMM_CUDA_TRY(cudaStreamSynchronize(st));
+    unsigned long long fl;
+    std::memcpy(&fl, &h[2], 8);
+    res->p_max = h[0] + (h[1] ? 1 : 0);
+    res->error_success = h[1] ? 0 : 1;
+    res->n_target_branches = T.n_branches;
+    res->n_source_branches = S.n_branches;
+    res->n_target_leaves = T.n_leaves;
+    res->n_source_leaves = S.n_leaves;
+    res->n_m2l = W.lists.n_m2l;
+    res->n_direct = W.lists.n_direct;
+    res->m2l_flops = (int64_t)fl;
+    res->n_p2p_pairs = -1;
+    if (timing) {
+      float ms[7];
+      for (int k = 0; k < 7; ++k) FMM_CUDA_TRY(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
+      res->t_tree_ms = ms[0];
+      res->t_lists_ms = ms[1] + ms[2];
+      res->t_nearfield_ms = ms[3];
+      res->t_upward_ms = ms[4];
+      res->t_horizontal_ms = ms[5];
+      res->t_downward_ms = ms[6];
+      float tot;
+      FMM_CUDA_TRY(cudaEventElapsedTime(&tot, ev[0], ev[7]));
+      res->t_total_ms = tot;
+    }
+  }
+  if (timing)
+    for (auto& e : ev) cudaEventDestroy(e);
+}
+
+void check_options(const fmm_options& o) {
+  FMM_CHECK(o.expansion_order >= 1 && o.expansion_order <= kMaxP, FMM_ERR_ARGUMENT,
+            "expansion_order must be in [1, 20]");
+  FMM_CHECK(o.leaf_size_source >= 1, FMM_ERR_ARGUMENT, "leaf_size_source must be >= 1");
+  FMM_CHECK(o.multipole_acceptance > 0, FMM_ERR_ARGUMENT, "multipole_acceptance must be > 0");
+  FMM_CHECK(o.error_method >= 0 && o.error_method <= 4, FMM_ERR_ARGUMENT, "unknown error_method");
+  FMM_CHECK(o.list_method >= 0 && o.list_method <= 2, FMM_ERR_ARGUMENT, "unknown list_method");
+  FMM_CHECK(o.precision == FMM_PRECISION_F64 || o.precision == FMM_PRECISION_MIXED, FMM_ERR_ARGUMENT,
+            "unknown precision");
+}
+
+void check_source(const fmm_source_system* s) {
+  FMM_CHECK(s != nullptr, FMM_ERR_ARGUMENT, "source system is NULL");
+  FMM_CHECK(s->kind == FMM_POINT_SOURCE || s->kind == FMM_POINT_VORTEX, FMM_ERR_ARGUMENT,
+            "source kind must be FMM_POINT_SOURCE or FMM_POINT_VORTEX");
+  FMM_CHECK(s->n_bodies >= 0, FMM_ERR_ARGUMENT, "negative n_bodies");
+  FMM_CHECK(s->data_per_body >= 4 + s->kind, FMM_ERR_ARGUMENT, "data_per_body too small for the strength");
+  FMM_CHECK(s->n_bodies == 0 || s->buffer, FMM_ERR_ARGUMENT, "source buffer is NULL");
+}
+
+// stage a caller buffer on the device (no copy for device memory)
+const double* stage(fmm_ctx* c, DevBuf<double>& buf, const double* ptr, size_t n_doubles, int memory) {
+  if (memory == FMM_MEMORY_DEVICE) return ptr;
+  buf.grow(n_doubles);
+  FMM_CUDA_TRY(cudaMemcpyAsync(buf.ptr, ptr, n_doubles * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  return buf.ptr;
+}
+
+size_t tree_bytes(const DevTree& t) {
+  return (t.body_start.cap + t.body_count.cap + t.child_start.cap + t.n_children.cap + t.parent.cap + t.i_leaf.cap +
+          t.level.cap + t.leaf_index.cap + t.sort_index.cap) *
+             4 +
+         (t.gcenter.cap + t.gbox.cap + t.gradius.cap + t.tcenter.cap + t.scenter.cap + t.tradius.cap + t.sradius.cap +
+          t.tbox.cap + t.sbox.cap + t.max_influence.cap + t.multipole.cap + t.local.cap) *
+             8 +
+         (t.pos.cap + t.str.cap) * 32;
+}
+
+size_t lists_bytes(const DevLists& l) {
+  return (l.m2l_t.cap + l.m2l_s.cap + l.dir_t.cap + l.dir_s.cap + l.m2l_tgt.cap + l.m2l_off.cap + l.dir_tgt.cap +
+          l.dir_off.cap) *
+         4;
+}
+
+template <class T>
+void rel(DevBuf<T>& b) {
+  b.release();
+}
+
+void release_tree(DevTree& t) {
+  rel(t.body_start); rel(t.body_count); rel(t.child_start); rel(t.n_children); rel(t.parent); rel(t.i_leaf);
+  rel(t.level); rel(t.gcenter); rel(t.gbox); rel(t.gradius); rel(t.tcenter); rel(t.scenter); rel(t.tradius);
+  rel(t.sradius); rel(t.tbox); rel(t.sbox); rel(t.max_influence); rel(t.leaf_index); rel(t.sort_index);
+  rel(t.pos); rel(t.str); rel(t.multipole); rel(t.local);
+}
+
+void release_lists(DevLists& l) {
+  rel(l.m2l_t); rel(l.m2l_s); rel(l.dir_t); rel(l.dir_s); rel(l.m2l_tgt); rel(l.m2l_off); rel(l.dir_tgt);
+  rel(l.dir_off);
+}
+
+void release_scratch(Scratch& s) {
+  rel(s.cub); rel(s.keys_a); rel(s.keys_b); rel(s.vals_a); rel(s.vals_b); rel(s.tmp_i); rel(s.tmp_j); rel(s.tmp_k);
+  rel(s.front_a); rel(s.front_b); rel(s.dir_raw); rel(s.m2l_raw); rel(s.cnt_a); rel(s.cnt_b); rel(s.counts);
+  rel(s.tmp_d); rel(s.staging); rel(s.out16); rel(s.flag);
+}
+
+}  // namespace
+
+extern "C" {
+
+void fmm_default_options(fmm_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->expansion_order = 5;
+  o->leaf_size_source = 20;
+  o->leaf_size_target = 0;
+  o->multipole_acceptance = 0.4;
+  o->error_method = FMM_ERROR_NONE;
+  o->error_tolerance = 0.0;
+  o->bonus_expansion = 1;
+  o->shrink_recenter = 1;
+  o->list_method = FMM_LIST_SELF_TUNING_TREE_STOP;
+  o->farfield = o->nearfield = o->self_induced = 1;
+  o->upward_pass = o->horizontal_pass = o->downward_pass = 1;
+  o->scalar_potential = 0;
+  o->gradient = 1;
+  o->hessian = 0;
+  o->precision = FMM_PRECISION_F64;
+}
+
+int fmm_ctx_create(fmm_ctx** out, int device) {
+  if (!out) return FMM_ERR_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0) return FMM_ERR_NO_DEVICE;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return FMM_ERR_NO_DEVICE;
+  if (prop.major != 10) return FMM_ERR_NO_DEVICE;  // built for sm_100a only
+  if (cudaSetDevice(device) != cudaSuccess) return FMM_ERR_CUDA;
+  fmm_ctx* c = new fmm_ctx();
+  c->device = device;
+  *out = c;
+  return FMM_OK;
+}
+
+int fmm_ctx_destroy(fmm_ctx* c) {
+  if (!c) return FMM_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (Workspace* w : {&c->main, &c->est}) {
+    release_tree(w->tree[0]);
+    release_tree(w->tree[1]);
+    release_lists(w->lists);
+    w->acc13.release();
+  }
+  release_scratch(c->sc);
+  c->tables.Hs.release();
+  c->tables.zeta.release();
+  c->tables.eta.release();
+  c->tables.Mt.release();
+  c->tables.Lt.release();
+  c->stage_s.release();
+  c->stage_t.release();
+  c->out16.release();
+  c->est_out16.release();
+  c->stats.release();
+  delete c;
+  return FMM_OK;
+}
+
+int fmm_ctx_set_stream(fmm_ctx* c, void* stream) {
+  if (!c) return FMM_ERR_ARGUMENT;
+  c->stream = reinterpret_cast<cudaStream_t>(stream);
+  return FMM_OK;
+}
+
+int fmm_ctx_set_timing(fmm_ctx* c, int enabled) {
+  if (!c) return FMM_ERR_ARGUMENT;
+  c->timing = enabled != 0;
+  return FMM_OK;
+}
+
+int fmm_ctx_set_hbm_budget(fmm_ctx* c, size_t bytes) {
+  if (!c) return FMM_ERR_ARGUMENT;
+  c->budget = bytes;
+  return FMM_OK;
+}
+
+size_t fmm_ctx_device_bytes(const fmm_ctx* c) {
+  if (!c) return 0;
+  size_t b = 0;
+  for (const Workspace* w : {&c->main, &c->est}) {
+    b += tree_bytes(w->tree[0]) + tree_bytes(w->tree[1]) + lists_bytes(w->lists) + w->acc13.cap * 8;
+  }
+  const Scratch& s = c->sc;
+  b += s.cub.cap + (s.keys_a.cap + s.keys_b.cap) * 8 +
+       (s.vals_a.cap + s.vals_b.cap + s.tmp_i.cap + s.tmp_j.cap + s.tmp_k.cap + s.cnt_a.cap + s.cnt_b.cap) * 4 +
+       (s.front_a.cap + s.front_b.cap + s.dir_raw.cap + s.m2l_raw.cap) * 8 + s.tmp_d.cap * 8;
+  b += (c->stage_s.cap + c->stage_t.cap + c->out16.cap + c->est_out16.cap) * 8;
+  return b;
+}
+
+const char* fmm_ctx_last_error(const fmm_ctx* c) { return c ? c->err.c_str() : "no context"; }
+
+int fmm_solve(fmm_ctx* c, const fmm_target_system* target, const fmm_source_system* source, const fmm_options* opt,
+              fmm_result* result) {
+  if (!c) return FMM_ERR_ARGUMENT;
+  try {
+    FMM_CHECK(opt != nullptr, FMM_ERR_ARGUMENT, "options are NULL");
+    check_options(*opt);
+    check_source(source);
+    FMM_CHECK(target != nullptr, FMM_ERR_ARGUMENT, "target system is NULL (it carries the output buffer)");
+    const bool self = target->positions == nullptr;  // fmm!(system): the sources are the targets
+    FMM_CHECK(self || target->stride >= 3, FMM_ERR_ARGUMENT, "target stride must be >= 3");
+    FMM_CUDA_TRY(cudaSetDevice(c->device));
+    if (result) std::memset(result, 0, sizeof(*result));
+    SolveIn in;
+    in.d = source->data_per_body;
+    in.kind = source->kind;
+    in.n_s = source->n_bodies;
+    in.src = nullptr;
+    in.tpos = nullptr;
+    in.t_stride = 0;
+    in.n_t = self ? source->n_bodies : target->n_bodies;
+    FMM_CHECK(in.n_t == 0 || target->out, FMM_ERR_ARGUMENT, "target out buffer is NULL");
+    FMM_CHECK(self || in.n_t == 0 || target->positions, FMM_ERR_ARGUMENT, "target positions are NULL");
+    if (c->budget) FMM_CHECK(footprint(in, *opt) <= c->budget, FMM_ERR_MEMORY, "request exceeds the context's HBM budget");
+    c->have_solve = false;
+    if (in.n_s == 0 || in.n_t == 0) {
+      // fmm! warns and foregoes the calculation (src/fmm.jl:1155-1158): rows 4..16 are zero
+      if (in.n_t > 0) {
+        if (target->memory == FMM_MEMORY_DEVICE) {
+          FMM_CUDA_TRY(cudaMemset2DAsync(target->out + 3, 16 * sizeof(double), 0, 13 * sizeof(double), in.n_t,
+                                         c->stream));
+          FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        } else {
+          for (int64_t i = 0; i < in.n_t; ++i) std::memset(target->out + 16 * i + 3, 0, 13 * sizeof(double));
+        }
+      }
+      if (result) result->error_success = 1;
+      return FMM_OK;
+    }
+    in.src = stage(c, c->stage_s, source->buffer, (size_t)in.d * in.n_s, source->memory);
+    if (!self) {
+      in.tpos = stage(c, c->stage_t, target->positions, (size_t)target->stride * target->n_bodies, target->memory);
+      in.t_stride = target->stride;
+    }
+    c->out16.grow(16 * (size_t)in.n_t);
+    run_fmm(c, c->main, in, *opt, c->out16.ptr, result, false);
+    // write the target buffer (rows 1..3 = positions, 4..16 = phi, gradient, hessian)
+    int mem = target->memory;
+    double* dst = target->out;
+    if (mem == FMM_MEMORY_DEVICE)
+      FMM_CUDA_TRY(cudaMemcpyAsync(dst, c->out16.ptr, 16 * in.n_t * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    else
+      FMM_CUDA_TRY(cudaMemcpyAsync(dst, c->out16.ptr, 16 * in.n_t * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->have_solve = true;
+    c->last_p = opt->expansion_order;
+    c->last_kind = source->kind;
+    return FMM_OK;
+  } catch (const Error& e) {
+    return fail(c, e);
+  }
+}
+
+int fmm_direct(fmm_ctx* c, const fmm_target_system* target, const fmm_source_system* source, int ps, int gs, int hs,
+               int precision) {
+  if (!c) return FMM_ERR_ARGUMENT;
+  try {
+    check_source(source);
+    FMM_CHECK(target != nullptr, FMM_ERR_ARGUMENT, "direct! needs a target buffer");
+    const bool self = target->positions == nullptr;
+    const int64_t nt = self ? source->n_bodies : target->n_bodies;
+    FMM_CHECK(self || target->stride >= 3, FMM_ERR_ARGUMENT, "target stride must be >= 3");
+    FMM_CHECK(nt == 0 || target->out, FMM_ERR_ARGUMENT, "target out buffer is NULL");
+    FMM_CHECK(precision == FMM_PRECISION_F64 || precision == FMM_PRECISION_MIXED, FMM_ERR_ARGUMENT,
+              "unknown precision");
+    FMM_CUDA_TRY(cudaSetDevice(c->device));
+    c->have_solve = false;
+    if (nt == 0) return FMM_OK;
+    const double* src = stage(c, c->stage_s, source->buffer, (size_t)source->data_per_body * source->n_bodies + 1,
+                              source->memory);
+    const double* tp = self ? src
+                            : stage(c, c->stage_t, target->positions, (size_t)target->stride * target->n_bodies,
+                                    target->memory);
+    DevTree& S = c->main.tree[1];
+    DevTree& T = c->main.tree[0];
+    unpack_bodies(S, src, source->n_bodies, source->data_per_body, source->kind, true, c->stream);
+    unpack_bodies(T, tp, nt, self ? source->data_per_body : target->stride, 0, false, c->stream);
+    c->main.acc13.grow(13 * (size_t)nt + 1);
+    FMM_CUDA_TRY(cudaMemsetAsync(c->main.acc13.ptr, 0, 13 * nt * sizeof(double), c->stream));
+    launch_direct(T.pos.ptr, nt, S.pos.ptr, S.str.ptr, source->n_bodies, c->main.acc13.ptr, source->kind, gs != 0,
+                  hs != 0, precision, c->stream);
+    (void)ps;
+    c->out16.grow(16 * (size_t)nt + 1);
+    k_unsort<<<grid_for(nt), 256, 0, c->stream>>>(c->main.acc13.ptr, nullptr, T.pos.ptr, nt, c->out16.ptr);
+    FMM_CUDA_TRY(cudaGetLastError());
+    auto kind = target->memory == FMM_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    FMM_CUDA_TRY(cudaMemcpyAsync(target->out, c->out16.ptr, 16 * nt * sizeof(double), kind, c->stream));
+    FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->have_solve = false;
+    return FMM_OK;
+  } catch (const Error& e) {
+    return fail(c, e);
+  }
+}
+
+int fmm_get_tree(fmm_ctx* c, int which, fmm_tree_view* v) {
+  if (!c || !v) return FMM_ERR_ARGUMENT;
+  try {
+    FMM_CHECK(c->have_solve, FMM_ERR_STATE, "no solve to export");
+    FMM_CHECK(which == 0 || which == 1, FMM_ERR_ARGUMENT, "which must be 0 (target) or 1 (source)");
+    DevTree& t = which == 0 ? c->main.target() : c->main.source();
+    const int64_t nb = t.n_branches;
+    v->n_branches = nb;
+    v->n_levels = t.n_levels;
+    v->n_leaves = t.n_leaves;
+    v->n_bodies = t.n_bodies;
+    FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    auto get_i = [&](const DevBuf<int>& d, int64_t n, int64_t* dst) {
+      if (!dst || n == 0) return;
+      std::vector<int> h(n);
+      FMM_CUDA_TRY(cudaMemcpy(h.data(), d.ptr, n * sizeof(int), cudaMemcpyDeviceToHost));
+      for (int64_t i = 0; i < n; ++i) dst[i] = h[i];
+    };
+    auto get_d = [&](const DevBuf<double>& d, int64_t n, double* dst) {
+      if (!dst || n == 0) return;
+      FMM_CUDA_TRY(cudaMemcpy(dst, d.ptr, n * sizeof(double), cudaMemcpyDeviceToHost));
+    };
+    get_i(t.body_start, nb, v->body_start);
+    get_i(t.body_count, nb, v->body_count);
+    get_i(t.child_start, nb, v->child_start);
+    get_i(t.n_children, nb, v->n_children);
+    get_i(t.parent, nb, v->parent);
+    get_i(t.i_leaf, nb, v->i_leaf);
+    get_d(t.tcenter, 3 * nb, v->target_center);
+    get_d(t.scenter, 3 * nb, v->source_center);
+    get_d(t.tradius, nb, v->target_radius);
+    get_d(t.sradius, nb, v->source_radius);
+    get_d(t.tbox, 3 * nb, v->target_box);
+    get_d(t.sbox, 3 * nb, v->source_box);
+    get_d(t.max_influence, nb, v->max_influence);
+    get_i(t.sort_index, t.n_bodies, v->sort_index);
+    get_i(t.leaf_index, t.n_leaves, v->leaf_index);
+    if (v->levels_start)
+      for (int l = 0; l < t.n_levels; ++l) v->levels_start[l] = t.levels_start[l];
+    if (v->levels_end)
+      for (int l = 0; l < t.n_levels; ++l) v->levels_end[l] = t.levels_end[l];
+    return FMM_OK;
+  } catch (const Error& e) {
+    return fail(c, e);
+  }
+}
+
+int fmm_get_lists(fmm_ctx* c, int32_t* m2l, int64_t* n_m2l, int32_t* direct, int64_t* n_direct) {
+  if (!c) return FMM_ERR_ARGUMENT;
+  try {
+    FMM_CHECK(c->have_solve, FMM_ERR_STATE, "no solve to export");
+    DevLists& L = c->main.lists;
+    if (n_m2l) *n_m2l = L.n_m2l;
+    if (n_direct) *n_direct = L.n_direct;
+    FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    auto pairs = [&](const DevBuf<int>& t, const DevBuf<int>& s, int64_t n, int32_t* dst) {
+      if (!dst || n == 0) return;
+      std::vector<int> ht(n), hs(n);
+      FMM_CUDA_TRY(cudaMemcpy(ht.data(), t.ptr, n * sizeof(int), cudaMemcpyDeviceToHost));
+      FMM_CUDA_TRY(cudaMemcpy(hs.data(), s.ptr, n * sizeof(int), cudaMemcpyDeviceToHost));
+      for (int64_t i = 0; i < n; ++i) {
+        dst[2 * i] = ht[i];
+        dst[2 * i + 1] = hs[i];
+      }
+    };
+    pairs(L.m2l_t, L.m2l_s, L.n_m2l, m2l);
+    pairs(L.dir_t, L.dir_s, L.n_direct, direct);
+    return FMM_OK;
+  } catch (const Error& e) {
+    return fail(c, e);
+  }
+}
+
+int fmm_get_expansions(fmm_ctx* c, int which, double* out, int64_t n_doubles) {
+  if (!c || !out) return FMM_ERR_ARGUMENT;
+  try {
+    FMM_CHECK(c->have_solve, FMM_ERR_STATE, "no solve to export");
+    DevTree& t = which == 0 ? c->main.target() : c->main.source();
+    const DevBuf<double>& e = which == 0 ? t.local : t.multipole;
+    int64_t need = 4 * nh(c->last_p) * t.n_branches;
+    FMM_CHECK(n_doubles >= need, FMM_ERR_ARGUMENT, "output too small for the expansions");
+    FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    FMM_CUDA_TRY(cudaMemcpy(out, e.ptr, need * sizeof(double), cudaMemcpyDeviceToHost));
+    return FMM_OK;
+  } catch (const Error& e) {
+    return fail(c, e);
+  }
+}
+
+// ---- single operators ----------------------------------------------------------
+int fmm_op_p2m(fmm_ctx* c, int kind, const double* buf, int d, int64_t n, const double* center, int p,
+               double* expansion) {
+  if (!c) return FMM_ERR_ARGUMENT;
+  try {
+    FMM_CHECK(p >= 1 && p <= kMaxP, FMM_ERR_ARGUMENT, "p must be in [1, 20]");
+    FMM_CHECK(kind == FMM_POINT_SOURCE || kind == FMM_POINT_VORTEX, FMM_ERR_ARGUMENT, "bad kind");
+    FMM_CHECK(d >= 4 + kind && n >= 0 && buf && center && expansion, FMM_ERR_ARGUMENT, "bad p2m arguments");
+    FMM_CUDA_TRY(cudaSetDevice(c->device));
+    const double* src = stage(c, c->stage_s, buf, (size_t)d * n + 1, FMM_MEMORY_HOST);
+    DevTree& S = c->main.tree[1];
+    unpack_bodies(S, src, n, d, kind, true, c->stream);
+    int64_t NH4 = 4 * nh(p);
+    c->sc.tmp_d.grow(NH4);
+    FMM_CUDA_TRY(cudaMemcpyAsync(c->sc.tmp_d.ptr, expansion, NH4 * 8, cudaMemcpyHostToDevice, c->stream));
+    launch_op_p2m(kind, S.pos.ptr, S.str.ptr, n, center, p, c->sc.tmp_d.ptr, c->stream);
+    FMM_CUDA_TRY(cudaMemcpyAsync(expansion, c->sc.tmp_d.ptr, NH4 * 8, cudaMemcpyDeviceToHost, c->stream));
+    FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->have_solve = false;
+    return FMM_OK;
+  } catch (const Error& e) {
+    return fail(c, e);
+  }
+}
+
+namespace {
+struct OpBufs {
+  DevBuf<double> a, b, cc, dd, e, f, g;
+  DevBuf<int> pu;
+  ~OpBufs() {
+    a.release(); b.release(); cc.release(); dd.release(); e.release(); f.release(); g.release(); pu.release();
+  }
+};
+double* up(DevBuf<double>& d, const double* h, size_t n, cudaStream_t st) {
+  if (!h) return nullptr;
+  d.grow(n);
+  FMM_CUDA_TRY(cudaMemcpyAsync(d.ptr, h, n * 8, cudaMemcpyHostToDevice, st));
+  return d.ptr;
+}
+}  // namespace
+
+static int op_pairs(fmm_ctx* c, int64_t n, double* target, const double* tc, const double* src, const double* sc,
+                    int p, int lh, bool local) {
+  if (!c) return FMM_ERR_ARGUMENT;
+  try {
+    FMM_CHECK(p >= 1 && p <= kMaxP, FMM_ERR_ARGUMENT, "p must be in [1, 20]");
+    FMM_CHECK(n >= 0 && target && tc && src && sc, FMM_ERR_ARGUMENT, "bad operator arguments");
+    FMM_CUDA_TRY(cudaSetDevice(c->device));
+    upload_tables(c->tables, p, c->stream);
+    OpBufs B;
+    size_t NH4 = 4 * nh(p);
+    double* dt = up(B.a, target, NH4 * n, c->stream);
+    double* dtc = up(B.b, tc, 3 * n, c->stream);
+    double* ds = up(B.cc, src, NH4 * n, c->stream);
+    double* dsc = up(B.dd, sc, 3 * n, c->stream);
+    launch_op_m2m(n, dt, dtc, ds, dsc, p, lh != 0, local, c->tables, c->stream);
+    FMM_CUDA_TRY(cudaMemcpyAsync(target, dt, NH4 * n * 8, cudaMemcpyDeviceToHost, c->stream));
+    FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return FMM_OK;
+  } catch (const Error& e) {
+    return fail(c, e);
+  }
+}
+
+int fmm_op_m2m(fmm_ctx* c, int64_t n, double* target, const double* tc, const double* src, const double* sc, int p,
+               int lh) {
+  return op_pairs(c, n, target, tc, src, sc, p, lh, false);
+}
+
+int fmm_op_l2l(fmm_ctx* c, int64_t n, double* target, const double* tc, const double* src, const double* sc, int p,
+               int lh) {
+  return op_pairs(c, n, target, tc, src, sc, p, lh, true);
+}
+
+int fmm_op_m2l(fmm_ctx* c, int64_t n, double* target, const double* tc, const double* tbox, const double* trad,
+               const double* maxinf, const double* src, const double* sc, int p, int lh, int em, double eps, int be,
+               int* p_used) {
+  if (!c) return FMM_ERR_ARGUMENT;
+  try {
+    FMM_CHECK(p >= 1 && p <= kMaxP, FMM_ERR_ARGUMENT, "p must be in [1, 20]");
+    FMM_CHECK(n >= 0 && target && tc && src && sc, FMM_ERR_ARGUMENT, "bad operator arguments");
+    FMM_CHECK(em >= 0 && em <= 4, FMM_ERR_ARGUMENT, "unknown error method");
+    FMM_CUDA_TRY(cudaSetDevice(c->device));
+    upload_tables(c->tables, p, c->stream);
+    OpBufs B;
+    size_t NH4 = 4 * nh(p);
+    double* dt = up(B.a, target, NH4 * n, c->stream);
+    double* dtc = up(B.b, tc, 3 * n, c->stream);
+    double* dtb = up(B.e, tbox, 3 * n, c->stream);
+    double* dtr = up(B.f, trad, n, c->stream);
+    double* dmi = up(B.g, maxinf, n, c->stream);
+    double* ds = up(B.cc, src, NH4 * n, c->stream);
+    double* dsc = up(B.dd, sc, 3 * n, c->stream);
+    int* dpu = nullptr;
+    if (p_used) {
+      B.pu.grow(n + 1);
+      dpu = B.pu.ptr;
+    }
+    launch_op_m2l(n, dt, dtc, dtb, dtr, dmi, ds, dsc, p, lh != 0, em, eps, be, dpu, c->tables, c->stream);
+    FMM_CUDA_TRY(cudaMemcpyAsync(target, dt, NH4 * n * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (p_used) FMM_CUDA_TRY(cudaMemcpyAsync(p_used, dpu, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return FMM_OK;
+  } catch (const Error& e) {
+    return fail(c, e);
+  }
+}
+
+int fmm_op_l2p(fmm_ctx* c, int64_t n, const double* dx, const double* local, int p, int lh, int ps, int gs, int hs,
+               double* out13) {
+  if (!c) return FMM_ERR_ARGUMENT;
+  try {
+    FMM_CHECK(p >= 1 && p <= kMaxP, FMM_ERR_ARGUMENT, "p must be in [1, 20]");
+    FMM_CHECK(n >= 0 && dx && local && out13, FMM_ERR_ARGUMENT, "bad operator arguments");
+    FMM_CUDA_TRY(cudaSetDevice(c->device));
+    OpBufs B;
+    double* ddx = up(B.a, dx, 3 * n, c->stream);
+    double* dl = up(B.b, local, 4 * nh(p), c->stream);
+    B.cc.grow(13 * n + 1);
+    FMM_CUDA_TRY(cudaMemsetAsync(B.cc.ptr, 0, 13 * n * 8, c->stream));
+    launch_op_l2p(n, ddx, dl, p, lh != 0, ps != 0, gs != 0, hs != 0, B.cc.ptr, c->stream);
+    FMM_CUDA_TRY(cudaMemcpyAsync(out13, B.cc.ptr, 13 * n * 8, cudaMemcpyDeviceToHost, c->stream));
+    FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return FMM_OK;
+  } catch (const Error& e) {
+    return fail(c, e);
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,236 @@
+"""GPU end-to-end parity through fmm_solve / fmm_direct against the FP64 oracle.
+
+* octree (permutation, branch ranges, centres, radii, boxes, leaf numbering) and the
+  interaction lists: bit-exact;
+* FP64 fmm! results: within 1e-10 of the oracle's, relative to the field's magnitude;
+* MIXED results: relative L2 error vs the FP64 all-pairs direct sum within the bound
+  the configuration states.
+"""
+import numpy as np
+import pytest
+
+import fastmultipole_b200 as fm
+from fastmultipole_b200 import _lib as L
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = fm.Context(0)
+    yield c
+    c.close()
+
+
+def uniform(n, seed, kind=1, radius=0.0):
+    rng = np.random.default_rng(seed)
+    d = 5 if kind == 1 else 7
+    b = np.zeros((n, d))
+    b[:, :3] = rng.random((n, 3))
+    b[:, 3] = radius * rng.random(n)
+    if kind == 1:
+        b[:, 4] = rng.random(n)
+    else:
+        b[:, 4:7] = (2 * rng.random((n, 3)) - 1) / n
+    return b
+
+
+def clustered(n, seed):
+    rng = np.random.default_rng(seed)
+    b = np.zeros((n, 5))
+    nb = n // 10
+    centres = rng.random((8, 3))
+    k = rng.integers(0, 8, n - nb)
+    b[: n - nb, :3] = centres[k] + 0.05 * rng.standard_normal((n - nb, 3))
+    b[n - nb:, :3] = rng.random((nb, 3))
+    b[:, 4] = 2 * rng.random(n) - 1
+    return b
+
+
+def ring(n, seed):
+    rng = np.random.default_rng(seed)
+    phi = 2 * np.pi * rng.random(n)
+    off = 0.05 * rng.standard_normal((n, 2))
+    R = 1.0 + off[:, 0]
+    b = np.zeros((n, 7))
+    b[:, 0] = R * np.cos(phi)
+    b[:, 1] = R * np.sin(phi)
+    b[:, 2] = off[:, 1]
+    t = np.stack([-np.sin(phi), np.cos(phi), np.zeros(n)], axis=1)
+    b[:, 4:7] = t / n + 1e-3 * rng.standard_normal((n, 3)) / n
+    return b
+
+
+def opt_pair(**kw):
+    o_gpu = fm.make_options(**{k: v for k, v in kw.items() if k != "n_threads"})
+    o_orc = O.options(expansion_order=o_gpu.expansion_order, leaf_size_source=o_gpu.leaf_size_source,
+                      leaf_size_target=o_gpu.leaf_size_target, multipole_acceptance=o_gpu.multipole_acceptance,
+                      error_method=o_gpu.error_method, error_tolerance=o_gpu.error_tolerance,
+                      bonus_expansion=o_gpu.bonus_expansion, shrink_recenter=o_gpu.shrink_recenter,
+                      list_method=o_gpu.list_method, farfield=o_gpu.farfield, nearfield=o_gpu.nearfield,
+                      self_induced=o_gpu.self_induced, scalar_potential=o_gpu.scalar_potential,
+                      gradient=o_gpu.gradient, hessian=o_gpu.hessian)
+    return o_gpu, o_orc
+
+
+def compare_trees(g, o):
+    assert g["n_branches"] == o["n_branches"]
+    for k in ("body_start", "body_count", "n_children", "parent", "i_leaf"):
+        np.testing.assert_array_equal(g[k], o[k], err_msg=k)
+    # child_start of leaves is the running counter in both implementations
+    np.testing.assert_array_equal(g["child_start"], o["child_start"])
+    np.testing.assert_array_equal(g["sort_index"], o["sort_index"])
+    np.testing.assert_array_equal(g["leaf_index"], o["leaf_index"])
+    np.testing.assert_array_equal(g["levels_start"], o["levels_start"])
+    for k in ("target_center", "source_center", "target_radius", "source_radius", "target_box", "source_box"):
+        np.testing.assert_array_equal(g[k], o[k], err_msg=k)
+
+
+def compare_lists(gm, gd, om, od):
+    # identical (target, source) pair sets, both sorted by target; order within a target may differ
+    for a, b in ((gm, om), (gd, od)):
+        assert len(a) == len(b)
+        np.testing.assert_array_equal(a[:, 0], b[:, 0])
+        ka = np.lexsort((a[:, 1], a[:, 0]))
+        kb = np.lexsort((b[:, 1], b[:, 0]))
+        np.testing.assert_array_equal(a[ka], b[kb])
+
+
+CASES = [
+    dict(name="uniform10k_p6_ls50", gen=lambda: uniform(10000, 1), kw=dict(expansion_order=6, leaf_size_source=50,
+                                                                            multipole_acceptance=0.5,
+                                                                            scalar_potential=True)),
+    dict(name="uniform_radius_barba", gen=lambda: uniform(6000, 2, radius=0.01),
+         kw=dict(expansion_order=5, leaf_size_source=30, multipole_acceptance=0.6,
+                 interaction_list_method=fm.Barba())),
+    dict(name="uniform_selftuning_noshrink", gen=lambda: uniform(5000, 3),
+         kw=dict(expansion_order=4, leaf_size_source=25, multipole_acceptance=0.4, shrink_recenter=False,
+                 interaction_list_method=fm.SelfTuning())),
+    dict(name="clustered20k_p10", gen=lambda: clustered(20000, 2),
+         kw=dict(expansion_order=10, leaf_size_source=64, multipole_acceptance=0.5)),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_tree_lists_and_fmm_match_oracle(ctx, case):
+    buf = case["gen"]()
+    og, oo = opt_pair(**case["kw"])
+    out, res = fm.solve_buffers(buf, L.FMM_POINT_SOURCE, og, ctx=ctx)
+    ref = O.fmm(buf, O.POINT_SOURCE, oo, want_tree=True)
+    compare_trees(fm.get_tree(ctx, 1), ref["source_tree"])
+    compare_trees(fm.get_tree(ctx, 0), ref["target_tree"])
+    gm, gd = fm.get_lists(ctx)
+    compare_lists(gm, gd, ref["m2l"], ref["direct"])
+    rows = slice(3, 7) if og.scalar_potential else slice(4, 7)
+    scale = np.abs(ref["out"][:, rows]).max()
+    np.testing.assert_allclose(out[:, rows], ref["out"][:, rows], rtol=0, atol=1e-10 * scale)
+    np.testing.assert_array_equal(out[:, :3], buf[:, :3])
+    assert res.p_max == ref["pmax"] or len(ref["m2l"]) == 0
+
+
+def test_vortex_ring_velocity_and_gradient(ctx):
+    buf = ring(20000, 3)
+    og, oo = opt_pair(expansion_order=12, leaf_size_source=80, multipole_acceptance=0.4, hessian=True)
+    out, res = fm.solve_buffers(buf, L.FMM_POINT_VORTEX, og, ctx=ctx)
+    ref = O.fmm(buf, O.POINT_VORTEX, oo, want_tree=True)
+    compare_trees(fm.get_tree(ctx, 1), ref["source_tree"])
+    for rows in (slice(4, 7), slice(7, 16)):
+        scale = np.abs(ref["out"][:, rows]).max()
+        np.testing.assert_allclose(out[:, rows], ref["out"][:, rows], rtol=0, atol=1e-10 * scale)
+
+
+@pytest.mark.parametrize("em", [fm.PowerRelativeGradient(1e-6), fm.PowerAbsoluteGradient(1e-4),
+                                fm.RotatedCoefficientsRelativeGradient(1e-6)], ids=["prg", "pag", "rcrg"])
+def test_error_controlled_orders_match_oracle(ctx, em):
+    buf = clustered(15000, 5)
+    og, oo = opt_pair(expansion_order=10, leaf_size_source=64, multipole_acceptance=0.5, error_tolerance=em)
+    out, res = fm.solve_buffers(buf, L.FMM_POINT_SOURCE, og, ctx=ctx)
+    ref = O.fmm(buf, O.POINT_SOURCE, oo, want_tree=True)
+    if em.code in (L.FMM_POWER_RELATIVE_GRADIENT, L.FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT):
+        g = fm.get_tree(ctx, 0)
+        np.testing.assert_allclose(g["max_influence"], ref["target_tree"]["max_influence"], rtol=1e-11, atol=0)
+    assert res.p_max == ref["pmax"]
+    assert bool(res.error_success) == ref["error_success"]
+    scale = np.abs(ref["out"][:, 4:7]).max()
+    np.testing.assert_allclose(out[:, 4:7], ref["out"][:, 4:7], rtol=0, atol=1e-10 * scale)
+
+
+def test_dual_tree_probes(ctx):
+    src = uniform(20000, 4)
+    rng = np.random.default_rng(44)
+    probes = -0.5 + 2.0 * rng.random((3000, 3))
+    og, oo = opt_pair(expansion_order=8, leaf_size_source=40, multipole_acceptance=0.5, scalar_potential=True)
+    out, res = fm.solve_buffers(src, L.FMM_POINT_SOURCE, og, target_pos=probes, ctx=ctx)
+    ref = O.fmm(src, O.POINT_SOURCE, oo, target_pos=probes, want_tree=True)
+    compare_trees(fm.get_tree(ctx, 0), ref["target_tree"])
+    scale = np.abs(ref["out"][:, 3:7]).max()
+    np.testing.assert_allclose(out[:, 3:7], ref["out"][:, 3:7], rtol=0, atol=1e-10 * scale)
+
+
+@pytest.mark.parametrize("kind", [1, 3])
+def test_direct_matches_oracle(ctx, kind):
+    buf = uniform(3000, 9, kind=kind)
+    tgt = np.zeros((3000, 16))
+    src = L.SourceSystem(kind, 3000, buf.shape[1], buf.ctypes.data, 0)
+    tsys = L.TargetSystem(3000, None, 0, tgt.ctypes.data, 0)
+    import ctypes as C
+    ctx.check(L.lib().fmm_direct(ctx.handle, C.byref(tsys), C.byref(src), 1, 1, 1, 0))
+    ref = O.direct(buf, kind, ps=1, gs=1, hs=1)
+    rows = slice(3, 7) if kind == 1 else slice(4, 16)
+    np.testing.assert_allclose(tgt[:, rows], ref[:, rows], rtol=0, atol=1e-12 * np.abs(ref[:, rows]).max())
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def test_mixed_precision_error_bounds(ctx):
+    buf = clustered(30000, 11)
+    og, _ = opt_pair(expansion_order=10, leaf_size_source=64, multipole_acceptance=0.5,
+                     error_tolerance=fm.PowerRelativeGradient(1e-6), precision="mixed")
+    out, _ = fm.solve_buffers(buf, L.FMM_POINT_SOURCE, og, ctx=ctx)
+    ids = np.random.default_rng(0).choice(len(buf), 2000, replace=False)
+    ref = O.direct_subset(buf, O.POINT_SOURCE, ids)
+    assert rel_l2(out[ids, 4:7], ref[:, 4:7]) < 1e-6
+
+
+def test_python_api_systems(ctx):
+    rng = np.random.default_rng(5)
+    n = 4000
+    sys_ = fm.PointSources(rng.random((n, 3)), rng.random(n) / n)
+    fm.fmm(sys_, expansion_order=12, leaf_size=30, multipole_acceptance=0.5, scalar_potential=True, context=ctx)
+    fmm_phi = sys_.potential[:, 0].copy()
+    fmm_grad = sys_.potential[:, 4:7].copy()
+    sys_.potential[:] = 0
+    fm.direct(sys_, scalar_potential=True, context=ctx)
+    np.testing.assert_allclose(fmm_phi, sys_.potential[:, 0], rtol=0, atol=1e-7 * np.abs(fmm_phi).max())
+    np.testing.assert_allclose(fmm_grad, sys_.potential[:, 4:7], rtol=0, atol=1e-6 * np.abs(fmm_grad).max())
+
+
+def test_empty_and_tiny_systems(ctx):
+    og, oo = opt_pair(expansion_order=4, leaf_size_source=10)
+    for n in (1, 2, 7):
+        buf = uniform(n, n)
+        out, res = fm.solve_buffers(buf, L.FMM_POINT_SOURCE, og, ctx=ctx)
+        ref = O.fmm(buf, O.POINT_SOURCE, oo)
+        np.testing.assert_allclose(out[:, 4:7], ref["out"][:, 4:7], rtol=1e-12, atol=1e-300)
+    out, res = fm.solve_buffers(np.zeros((0, 5)), L.FMM_POINT_SOURCE, og, target_pos=np.random.rand(5, 3), ctx=ctx)
+    assert np.all(out[:, 3:] == 0)
+
+
+def test_invalid_arguments_are_errors_not_faults(ctx):
+    buf = uniform(100, 1)
+    og, _ = opt_pair(expansion_order=40)
+    with pytest.raises(fm.FMMError) as e:
+        fm.solve_buffers(buf, L.FMM_POINT_SOURCE, og, ctx=ctx)
+    assert e.value.status == L.FMM_ERR_ARGUMENT
+    og, _ = opt_pair(expansion_order=4, leaf_size_source=1)
+    dup = np.zeros((50, 5))
+    dup[:, 4] = 1.0  # coincident bodies: the octree cannot separate them
+    with pytest.raises(fm.FMMError) as e:
+        fm.solve_buffers(dup, L.FMM_POINT_SOURCE, og, ctx=ctx)
+    assert e.value.status == L.FMM_ERR_TREE_DEPTH
+    # the context stays usable
+    out, _ = fm.solve_buffers(buf, L.FMM_POINT_SOURCE, fm.make_options(expansion_order=4), ctx=ctx)
+    assert np.isfinite(out).all()
