@@ -508,12 +508,15 @@ int fmm_get_tree(fmm_ctx* c, int which, fmm_tree_view* v) {
     get_i(t.n_children, nb, v->n_children);
     get_i(t.parent, nb, v->parent);
     get_i(t.i_leaf, nb, v->i_leaf);
+    // The reference's target tree reads body radii from its target buffer, where
+    // that row is zero, so its source centre/box/radius equal the target ones.
+    const bool target_role = (which == 0);
     get_d(t.tcenter, 3 * nb, v->target_center);
-    get_d(t.scenter, 3 * nb, v->source_center);
+    get_d(target_role ? t.tcenter : t.scenter, 3 * nb, v->source_center);
     get_d(t.tradius, nb, v->target_radius);
-    get_d(t.sradius, nb, v->source_radius);
+    get_d(target_role ? t.tradius : t.sradius, nb, v->source_radius);
     get_d(t.tbox, 3 * nb, v->target_box);
-    get_d(t.sbox, 3 * nb, v->source_box);
+    get_d(target_role ? t.tbox : t.sbox, 3 * nb, v->source_box);
     get_d(t.max_influence, nb, v->max_influence);
     get_i(t.sort_index, t.n_bodies, v->sort_index);
     get_i(t.leaf_index, t.n_leaves, v->leaf_index);
