@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 FMM evaluation path (one JSON line on rank 0).
+
+Default workload (the headline configuration): N = 1,000,000 Laplace point
+sources in 8 isotropic Gaussian clusters (sigma 0.05, centres uniform in the
+unit cube) plus 10% uniform background, strengths uniform in [-1, 1], seed 2;
+expansion_order 10, leaf_size 64, multipole_acceptance 0.5,
+PowerRelativeGradient(1e-6); potential and gradient at every body.  A step is
+one fmm! (tree, lists, influence estimate, all passes, unsort).
+
+* value   : bodies/s of the MIXED-precision solve with inputs resident in HBM
+* e2e     : bodies/s through fmm_solve with pinned host buffers (H2D of the
+            source buffer and D2H of the 16-row target buffer inside each step)
+* f64_*   : the same for the plain FP64 drop-in
+* rel_err : relative L2 error of the gradient vs FP64 all-pairs direct on a
+            20,000-target subsample
+Multi-GPU (torchrun): independent replicas, one per GPU ("scaling": "weak").
+`--impl reference` times the CPU restatement of the reference algorithm (the
+Julia package cannot run on this image) on all host cores.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+# ---------------------------------------------------------------------------
+# synthetic workloads (seeded; shapes and distributions of the configurations)
+def gen_uniform(n, seed):
+    rng = np.random.default_rng(seed)
+    b = np.zeros((n, 5))
+    b[:, :3] = rng.random((n, 3))
+    b[:, 4] = rng.random(n)
+    return b
+
+
+def gen_clustered(n, seed):
+    rng = np.random.default_rng(seed)
+    b = np.zeros((n, 5))
+    nb = n // 10
+    centres = rng.random((8, 3))
+    k = rng.integers(0, 8, n - nb)
+    b[: n - nb, :3] = centres[k] + 0.05 * rng.standard_normal((n - nb, 3))
+    b[n - nb:, :3] = rng.random((nb, 3))
+    b[:, 4] = 2 * rng.random(n) - 1
+    return b
+
+
+def gen_ring(n, seed):
+    rng = np.random.default_rng(seed)
+    phi = 2 * np.pi * rng.random(n)
+    off = 0.05 * rng.standard_normal((n, 2))
+    R = 1.0 + off[:, 0]
+    b = np.zeros((n, 7))
+    b[:, 0] = R * np.cos(phi)
+    b[:, 1] = R * np.sin(phi)
+    b[:, 2] = off[:, 1]
+    t = np.stack([-np.sin(phi), np.cos(phi), np.zeros(n)], axis=1)
+    b[:, 4:7] = t / n + 1e-3 * rng.standard_normal((n, 3)) / n
+    return b
+
+
+METRIC = "FMM bodies/sec at <=1e-6 rel err vs FP64 direct, mixed vs FP64"
+
+WORKLOADS = {
+    "c2": dict(workload="clustered-8-gaussian point sources N=1e6 (10% uniform), p<=10, leaf 64, MAC 0.5, "
+                        "PowerRelativeGradient(1e-6)",
+               n=1_000_000, gen=gen_clustered, seed=2, kind=1, p=10, ls=64, mac=0.5, err=1e-6,
+               ps=True, gs=True, hs=False, flops_per_pair=20, n_cpu=100_000),
+    "c1": dict(workload="uniform point sources N=1e4, p=6, leaf 50, MAC 0.5", n=10_000, gen=gen_uniform, seed=1,
+               kind=1, p=6, ls=50, mac=0.5, err=None, ps=True, gs=True, hs=False, flops_per_pair=20,
+               n_cpu=10_000),
+    "c3": dict(workload="vortex ring N=2e6 (R=1, core sigma 0.05), p=12, leaf 80, MAC 0.4, velocity + gradient",
+               n=2_000_000, gen=gen_ring, seed=3, kind=3, p=12, ls=80, mac=0.4, err=None, ps=False, gs=True,
+               hs=True, flops_per_pair=72, n_cpu=40_000),
+}
+
+
+def options(fm, w, precision):
+    err = fm.PowerRelativeGradient(w["err"]) if w["err"] else None
+    return fm.make_options(expansion_order=w["p"], leaf_size_source=w["ls"], multipole_acceptance=w["mac"],
+                           error_tolerance=err, scalar_potential=w["ps"], gradient=w["gs"], hessian=w["hs"],
+                           precision=precision)
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU: the restatement of the reference algorithm on all host cores
+def cpu_run(w, n, seed):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    buf = w["gen"](n, seed)
+    em = O.ERR_POWER_REL_GRAD if w["err"] else O.ERR_NONE
+    o = O.options(expansion_order=w["p"], leaf_size_source=w["ls"], multipole_acceptance=w["mac"], error_method=em,
+                  error_tolerance=w["err"] or 0.0, scalar_potential=int(w["ps"]), gradient=int(w["gs"]),
+                  hessian=int(w["hs"]), n_threads=0)
+    t0 = time.perf_counter()
+    O.fmm(buf, w["kind"], o)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(w, n=None):
+    n = n or w["n_cpu"]
+    dt = cpu_run(w, n, w["seed"] + 1000)
+    return {"value": n / dt, "unit": "bodies/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{n:,} bodies of the same distribution, one fmm! of the C++ FP64 restatement, {dt:.2f} s"}
+
+
+def reference_arm(args, w, rank):
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        cpu_run(w, w["n_cpu"], w["seed"] + 1000)
+    ts = [cpu_run(w, w["n_cpu"], w["seed"] + 1000) for _ in range(args.steps)]
+    v = w["n_cpu"] / (sum(ts) / len(ts))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "bodies/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(ts) / len(ts),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w["workload"], "sample_bodies": w["n_cpu"]},
+            "cpu_baseline": {"value": v, "unit": "bodies/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"{w['n_cpu']:,} bodies of the workload's distribution per step; the Julia "
+                                       "reference itself is unavailable on this image"},
+            "e2e": {"value": v, "unit": "bodies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def gpu_arm(args, w, rank, world, local_rank):
+    import torch
+    import fastmultipole_b200 as fm
+    from fastmultipole_b200 import _lib as L
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream(dev)
+    ctx = fm.Context(local_rank)
+    ctx.set_stream(stream.cuda_stream)
+    lib = L.lib()
+    n, kind = w["n"], w["kind"]
+    buf = w["gen"](n, w["seed"])
+    d = buf.shape[1]
+    src_dev = torch.from_numpy(buf).to(dev)
+    out_dev = torch.empty((n, 16), dtype=torch.float64, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    src_d = L.SourceSystem(kind, n, d, src_dev.data_ptr(), L.FMM_MEMORY_DEVICE)
+    tgt_d = L.TargetSystem(n, None, 0, out_dev.data_ptr(), L.FMM_MEMORY_DEVICE)
+    buf_pin = torch.from_numpy(buf).pin_memory()
+    out_pin = torch.empty((n, 16), dtype=torch.float64).pin_memory()
+    src_h = L.SourceSystem(kind, n, d, buf_pin.data_ptr(), L.FMM_MEMORY_HOST)
+    tgt_h = L.TargetSystem(n, None, 0, out_pin.data_ptr(), L.FMM_MEMORY_HOST)
+    res = L.Result()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(dev)
+
+    def timed(opt, src, tgt, steps, warmup):
+        ctx.set_timing(False)
+        for _ in range(warmup):
+            ctx.check(lib.fmm_solve(ctx.handle, C.byref(tgt), C.byref(src), C.byref(opt), C.byref(res)))
+        barrier()
+        total = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.check(lib.fmm_solve(ctx.handle, C.byref(tgt), C.byref(src), C.byref(opt), C.byref(res)))
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        barrier()
+        t = torch.tensor([total], dtype=torch.float64, device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item()) / steps  # ms per step, max over ranks
+
+    opt_mixed = options(fm, w, "mixed")
+    opt_f64 = options(fm, w, "f64")
+    with ClockSampler(local_rank) as clk:
+        ms_mixed = timed(opt_mixed, src_d, tgt_d, args.steps, args.warmup)
+    launches = res.n_kernel_launches
+    ms_f64 = timed(opt_f64, src_d, tgt_d, args.steps, max(1, args.warmup // 2))
+    ms_e2e = timed(opt_mixed, src_h, tgt_h, args.steps, 1)
+
+    # stage times of one solve (roofline of the dominant kernel)
+    def staged(opt):
+        ctx.set_timing(True)
+        flush.zero_()
+        ctx.check(lib.fmm_solve(ctx.handle, C.byref(tgt_d), C.byref(src_d), C.byref(opt), C.byref(res)))
+        ctx.set_timing(False)
+        return {k: getattr(res, k) for k, _ in L.Result._fields_}
+
+    st_mixed = staged(opt_mixed)
+    st_f64 = staged(opt_f64)
+
+    # accuracy vs FP64 all-pairs direct on a 20k-target subsample
+    ids = np.random.default_rng(7).choice(n, min(n, 20_000), replace=False)
+    tpos = np.ascontiguousarray(buf[ids, :3])
+    ref = np.zeros((len(ids), 16))
+    tsub = L.TargetSystem(len(ids), tpos.ctypes.data, 3, ref.ctypes.data, L.FMM_MEMORY_HOST)
+    ctx.check(lib.fmm_direct(ctx.handle, C.byref(tsub), C.byref(src_d), 1, 1, 0, L.FMM_PRECISION_F64))
+    errs = {}
+    for name, opt in (("mixed", opt_mixed), ("f64", opt_f64)):
+        ctx.check(lib.fmm_solve(ctx.handle, C.byref(tgt_d), C.byref(src_d), C.byref(opt), C.byref(res)))
+        got = out_dev.cpu().numpy()[ids]
+        rows = slice(4, 7)
+        errs[name] = float(np.linalg.norm(got[:, rows] - ref[:, rows]) / np.linalg.norm(ref[:, rows]))
+
+    if rank != 0:
+        return
+    pk = peaks()
+    sm_max = pk.get("sm_max_mhz", 1965.0)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    fp32_peak = sms * 128 * 2 * sm_max * 1e6 / 1e12
+    fp64_peak = fp32_peak / 2
+    near_flops = st_mixed["n_p2p_pairs"] * w["flops_per_pair"]
+    stages = {"nearfield": st_mixed["t_nearfield_ms"], "horizontal": st_mixed["t_horizontal_ms"],
+              "upward": st_mixed["t_upward_ms"], "downward": st_mixed["t_downward_ms"],
+              "tree": st_mixed["t_tree_ms"], "lists": st_mixed["t_lists_ms"]}
+    dom = max(("nearfield", "horizontal"), key=lambda k: stages[k])
+    if dom == "nearfield":
+        ach = near_flops / (stages["nearfield"] * 1e-3) / 1e12
+        roof = {"kernel": "k_p2p (FP32, mixed)", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": None,
+                "work": f"{st_mixed['n_p2p_pairs']:.3e} pairs x {w['flops_per_pair']} flop",
+                "peak_source": f"nominal FP32 CUDA-core peak, {sms} SMs x 128 lanes x 2 x {sm_max:.0f} MHz "
+                               "(MEASURED_PEAKS.json holds no CUDA-core figure)"}
+    else:
+        ach = st_mixed["m2l_flops"] / (stages["horizontal"] * 1e-3) / 1e12
+        roof = {"kernel": "k_m2l (FP64)", "bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": ach / fp64_peak, "traffic": None, "work": f"{st_mixed['m2l_flops']:.3e} algorithmic flop",
+                "peak_source": "nominal FP64 CUDA-core peak (half the FP32 rate)"}
+    value = world * n / (ms_mixed * 1e-3)
+    line = {
+        "metric": METRIC,
+        "value": value, "unit": "bodies/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": w["workload"], "n_bodies": n, "precision": "mixed", "parallelism": f"replicas x{world}",
+                   "l2": "256 MB buffer written between timed steps"},
+        "rel_err_vs_direct": errs["mixed"], "f64_rel_err_vs_direct": errs["f64"],
+        "f64_value": world * n / (ms_f64 * 1e-3), "f64_ms_per_step": ms_f64,
+        "speedup_mixed_vs_f64": ms_f64 / ms_mixed,
+        "e2e": {"value": world * n / (ms_e2e * 1e-3), "unit": "bodies/s", "ms_per_step": ms_e2e,
+                "h2d_bytes_per_step": int(buf.nbytes), "d2h_bytes_per_step": int(n * 16 * 8)},
+        "gpu_launches": int(launches) * args.steps,
+        "stages_ms": stages, "f64_stages_ms": {"nearfield": st_f64["t_nearfield_ms"],
+                                               "horizontal": st_f64["t_horizontal_ms"],
+                                               "upward": st_f64["t_upward_ms"], "downward": st_f64["t_downward_ms"],
+                                               "tree": st_f64["t_tree_ms"], "lists": st_f64["t_lists_ms"]},
+        "p_max": st_mixed["p_max"], "n_m2l": st_mixed["n_m2l"], "n_direct": st_mixed["n_direct"],
+        "n_p2p_pairs": st_mixed["n_p2p_pairs"],
+        "roofline": roof,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(w)
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    w = WORKLOADS[args.config]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, w, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        gpu_arm(args, w, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

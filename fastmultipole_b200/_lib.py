@@ -57,7 +57,7 @@ class Result(C.Structure):
                 ("m2l_flops", C.c_int64),
                 ("t_total_ms", C.c_double), ("t_tree_ms", C.c_double), ("t_lists_ms", C.c_double),
                 ("t_nearfield_ms", C.c_double), ("t_upward_ms", C.c_double), ("t_horizontal_ms", C.c_double),
-                ("t_downward_ms", C.c_double)]
+                ("t_downward_ms", C.c_double), ("n_kernel_launches", C.c_int64)]
 
 
 class TreeView(C.Structure):

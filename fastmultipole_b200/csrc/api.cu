@@ -97,6 +97,7 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   const int64_t ls_s = o.leaf_size_source;
   const int64_t ls_t = o.leaf_size_target > 0 ? o.leaf_size_target : ls_s;
   const bool ps = o.scalar_potential != 0, gs = o.gradient != 0, hs = o.hessian != 0;
+  const int64_t launches0 = g_launches;
   cudaEvent_t ev[8] = {};
   const bool timing = c->timing && !is_estimate && res;
   if (timing)
@@ -158,6 +159,7 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   FMM_CUDA_TRY(cudaMemsetAsync(W.acc13.ptr, 0, 13 * T.n_bodies * sizeof(double), st));
   c->stats.grow(8);
   FMM_CUDA_TRY(cudaMemsetAsync(c->stats.ptr, 0, 8 * sizeof(int), st));
+  count_p2p_pairs(T, S, W.lists, reinterpret_cast<unsigned long long*>(c->stats.ptr + 4), st);
   launch_p2p(T, S, W.lists, W.acc13.ptr, in.kind, ps, gs, hs, o.precision, st);
   mark(4);
   if (o.upward_pass) {
@@ -174,15 +176,17 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
     launch_l2p(T, p, lh, ps, gs, hs, W.acc13.ptr, st);
   }
   // ---- unsort into the caller's order (buffer_to_target!, src/compatibility.jl:324-338)
+  note_launch();
   k_unsort<<<grid_for(T.n_bodies), 256, 0, st>>>(W.acc13.ptr, T.sort_index.ptr, T.pos.ptr, T.n_bodies, out16);
   FMM_CUDA_TRY(cudaGetLastError());
   mark(7);
   if (res) {
-    int h[4] = {0, 0, 0, 0};
-    FMM_CUDA_TRY(cudaMemcpyAsync(h, c->stats.ptr, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    int h[6] = {0, 0, 0, 0, 0, 0};
+    FMM_CUDA_TRY(cudaMemcpyAsync(h, c->stats.ptr, 6 * sizeof(int), cudaMemcpyDeviceToHost, st));
     FMM_CUDA_TRY(cudaStreamSynchronize(st));
-    unsigned long long fl;
+    unsigned long long fl, pairs;
     std::memcpy(&fl, &h[2], 8);
+    std::memcpy(&pairs, &h[4], 8);
     res->p_max = h[0] + (h[1] ? 1 : 0);
     res->error_success = h[1] ? 0 : 1;
     res->n_target_branches = T.n_branches;
@@ -192,7 +196,8 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
     res->n_m2l = W.lists.n_m2l;
     res->n_direct = W.lists.n_direct;
     res->m2l_flops = (int64_t)fl;
-    res->n_p2p_pairs = -1;
+    res->n_p2p_pairs = (int64_t)pairs;
+    res->n_kernel_launches = g_launches - launches0;
     if (timing) {
       float ms[7];
       for (int k = 0; k < 7; ++k) FMM_CUDA_TRY(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
@@ -468,6 +473,7 @@ int fmm_direct(fmm_ctx* c, const fmm_target_system* target, const fmm_source_sys
                   hs != 0, precision, c->stream);
     (void)ps;
     c->out16.grow(16 * (size_t)nt + 1);
+    note_launch();
     k_unsort<<<grid_for(nt), 256, 0, c->stream>>>(c->main.acc13.ptr, nullptr, T.pos.ptr, nt, c->out16.ptr);
     FMM_CUDA_TRY(cudaGetLastError());
     auto kind = target->memory == FMM_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;

@@ -22,6 +22,10 @@ __host__ __device__ inline int64_t length_Ts(int p) { return p < 0 ? 0 : (int64_
 __host__ __device__ inline int H_index(int mp, int m) { return m * (m + 1) / 2 + mp; }
 __host__ __device__ inline int T_index(int mp, int m) { return m * m + mp + m; }
 
+// Kernel launches issued by this host thread (reported per solve in fmm_result).
+inline thread_local int64_t g_launches = 0;
+inline void note_launch() { ++g_launches; }
+
 // Status plumbing: every entry point returns an fmm_status and never aborts.
 struct Error {
   int code;

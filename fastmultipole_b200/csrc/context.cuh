@@ -86,6 +86,9 @@ void build_lists(DevLists& L, const DevTree& tt, const DevTree& stt, Scratch& sc
 // Near field over the direct list; accumulates into acc13 (sorted target order, 13 per body).
 void launch_p2p(const DevTree& tt, const DevTree& stt, const DevLists& L, double* acc13, int kind, bool ps,
                 bool gs, bool hs, int precision, cudaStream_t st);
+// sum over the direct list of n_target * n_source (atomically added to *out)
+void count_p2p_pairs(const DevTree& tt, const DevTree& stt, const DevLists& L, unsigned long long* out,
+                     cudaStream_t st);
 // All pairs (direct!): targets in pos order, sources; writes acc13.
 void launch_direct(const double4* tpos, int64_t nt, const double4* spos, const double4* sstr, int64_t ns,
                    double* acc13, int kind, bool gs, bool hs, int precision, cudaStream_t st);

@@ -1269,6 +1269,7 @@ void launch_p2m(DevTree& s, int p, int kind, const DevTables&, cudaStream_t st) 
   size_t sm = (size_t)kWarps * 2 * nh(p) * sizeof(double);
   allow_smem(k_p2m, sm);
   int g = (int)((s.n_leaves + kWarps - 1) / kWarps);
+  note_launch();
   k_p2m<<<g, 32 * kWarps, sm, st>>>(s.leaf_index.ptr, (int)s.n_leaves, s.body_start.ptr, s.body_count.ptr,
                                     s.scenter.ptr, s.pos.ptr, s.str.ptr, s.multipole.ptr, p, kind);
   FMM_CUDA_TRY(cudaGetLastError());
@@ -1280,6 +1281,7 @@ void launch_m2m(DevTree& s, int p, bool lh, const DevTables& tb, cudaStream_t st
   for (int l = s.n_levels - 2; l >= 0; --l) {
     int l0 = (int)s.levels_start[l], l1 = (int)s.levels_end[l];
     int g = (l1 - l0 + kWarps - 1) / kWarps;
+    note_launch();
     k_m2m<<<g, 32 * kWarps, sm, st>>>(l0, l1, s.child_start.ptr, s.n_children.ptr, s.scenter.ptr, s.multipole.ptr, p,
                                       lh ? 1 : 0, tab_of(tb));
   }
@@ -1294,6 +1296,7 @@ void launch_m2l(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh,
   int g = (int)((L.n_m2l_targets + kWarps - 1) / kWarps);
   // stats: [0] = max order used, [1] = any tolerance missed, [2..3] = flop count (u64)
   M2LStats S{stats, stats + 1, reinterpret_cast<unsigned long long*>(stats + 2)};
+  note_launch();
   k_m2l<<<g, 32 * kWarps, sm, st>>>(L.m2l_tgt.ptr, L.m2l_off.ptr, L.m2l_s.ptr, (int)L.n_m2l_targets, t.local.ptr,
                                     s.multipole.ptr, t.tcenter.ptr, t.tbox.ptr, t.tradius.ptr, t.max_influence.ptr,
                                     s.scenter.ptr, p, lh ? 1 : 0, em, eps, be, p_used, tab_of(tb), S);
@@ -1306,6 +1309,7 @@ void launch_l2l(DevTree& t, int p, bool lh, const DevTables& tb, cudaStream_t st
   for (int l = 1; l < t.n_levels; ++l) {
     int c0 = (int)t.levels_start[l], c1 = (int)t.levels_end[l];
     int g = (c1 - c0 + kWarps - 1) / kWarps;
+    note_launch();
     k_l2l<<<g, 32 * kWarps, sm, st>>>(c0, c1, t.parent.ptr, t.tcenter.ptr, t.local.ptr, p, lh ? 1 : 0,
                                       tab_of(tb));
   }
@@ -1316,6 +1320,7 @@ void launch_l2p(DevTree& t, int p, bool lh, bool ps, bool gs, bool hs, double* a
   if (t.n_leaves == 0) return;
   size_t sm = l2p_smem(p);
   allow_smem(k_l2p, sm);
+  note_launch();
   k_l2p<<<(int)t.n_leaves, kL2PThreads, sm, st>>>(t.leaf_index.ptr, t.body_start.ptr, t.body_count.ptr,
                                                    t.tcenter.ptr, t.pos.ptr, t.local.ptr, p, lh ? 1 : 0,
                                                    ps ? 1 : 0, gs ? 1 : 0, hs ? 1 : 0, acc13);
@@ -1327,6 +1332,7 @@ void launch_op_m2m(int64_t n, double* target, const double* tc, const double* sr
   if (n == 0) return;
   size_t sm = pair_smem(p);
   allow_smem(k_op_pairs, sm);
+  note_launch();
   k_op_pairs<<<(int)((n + kWarps - 1) / kWarps), 32 * kWarps, sm, st>>>(n, target, tc, src, sc, p, lh ? 1 : 0,
                                                                         local ? 1 : 0, tab_of(tb));
   FMM_CUDA_TRY(cudaGetLastError());
@@ -1338,6 +1344,7 @@ void launch_op_m2l(int64_t n, double* target, const double* tc, const double* tb
   if (n == 0) return;
   size_t sm = pair_smem(p);
   allow_smem(k_op_m2l, sm);
+  note_launch();
   k_op_m2l<<<(int)((n + kWarps - 1) / kWarps), 32 * kWarps, sm, st>>>(n, target, tc, tbox, trad, maxinf, src, sc, p,
                                                                       lh ? 1 : 0, em, eps, be, p_used, tab_of(tb));
   FMM_CUDA_TRY(cudaGetLastError());
@@ -1346,6 +1353,7 @@ void launch_op_m2l(int64_t n, double* target, const double* tc, const double* tb
 void launch_op_p2m(int kind, const double4* pos, const double4* str, int64_t n, const double* center, int p,
                    double* expansion, cudaStream_t st) {
   size_t sm = 2 * nh(p) * sizeof(double);
+  note_launch();
   k_op_p2m<<<1, 32, sm, st>>>(pos, str, n, center[0], center[1], center[2], expansion, p, kind);
   FMM_CUDA_TRY(cudaGetLastError());
 }
@@ -1356,6 +1364,7 @@ void launch_op_l2p(int64_t n, const double* dx, const double* local, int p, bool
   size_t sm = l2p_smem(p);
   allow_smem(k_op_l2p, sm);
   int g = (int)std::min<int64_t>((n + kL2PThreads - 1) / kL2PThreads, 1024);
+  note_launch();
   k_op_l2p<<<g, kL2PThreads, sm, st>>>(n, dx, local, p, lh ? 1 : 0, ps ? 1 : 0, gs ? 1 : 0, hs ? 1 : 0, out13);
   FMM_CUDA_TRY(cudaGetLastError());
 }

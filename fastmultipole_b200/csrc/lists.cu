@@ -164,6 +164,7 @@ void finish_list(DevBuf<int2>& raw, int64_t n, int nbits, DevBuf<int>& out_t, De
   }
   sc.tmp_i.grow(n);
   sc.tmp_j.grow(n);
+  note_launch();
   k_split<<<(int)((n + 255) / 256), 256, 0, st>>>(raw.ptr, (int)n, sc.tmp_i.ptr, sc.tmp_j.ptr);
   size_t tb = 0;
   unsigned int* ki = reinterpret_cast<unsigned int*>(sc.tmp_i.ptr);
@@ -216,6 +217,7 @@ void build_lists(DevLists& L, const DevTree& tt, const DevTree& stt, Scratch& sc
     Cnt3* cnt = reinterpret_cast<Cnt3*>(sc.cnt_a.ptr);
     Cnt3* off = reinterpret_cast<Cnt3*>(sc.cnt_b.ptr);
     int g = (nfront + 1 + 255) / 256;
+    note_launch();
     k_classify<<<g, 256, 0, st>>>(sc.front_a.ptr, nfront, T, S, R, cnt);
     size_t tb = 0;
     cub::DeviceScan::ExclusiveScan(nullptr, tb, cnt, off, Cnt3Sum(), Cnt3{0, 0, 0}, nfront + 1, st);
@@ -228,6 +230,7 @@ void build_lists(DevLists& L, const DevTree& tt, const DevTree& stt, Scratch& sc
     grow_keep_l(dir_raw, (size_t)(n_dir + tot.d + 1), st);
     grow_keep_l(m2l_raw, (size_t)(n_m2l + tot.m + 1), st);
     sc.front_b.grow((size_t)tot.n + 1);
+    note_launch();
     k_emit<<<(nfront + 255) / 256, 256, 0, st>>>(sc.front_a.ptr, nfront, T, S, R, off, dir_raw.ptr, (int)n_dir,
                                                  m2l_raw.ptr, (int)n_m2l, sc.front_b.ptr);
     FMM_CUDA_TRY(cudaGetLastError());

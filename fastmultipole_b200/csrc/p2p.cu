@@ -11,6 +11,8 @@
 // the MIXED variant moves every body relative to the target leaf centre in
 // FP64, then evaluates the kernel in FP32 (rsqrt on the SFU), summing each
 // source leaf in FP32 and the leaf partials in FP64.
+#include <algorithm>
+
 #include "context.cuh"
 
 namespace fmmb {
@@ -254,6 +256,7 @@ __global__ void __launch_bounds__(kP2PThreads) k_direct(const double4* __restric
 template <class R, int KIND, bool PS, bool GS, bool HS>
 void run_p2p(const DevTree& tt, const DevTree& stt, const DevLists& L, double* acc13, cudaStream_t st) {
   if (L.n_dir_targets == 0) return;
+  note_launch();
   k_p2p<R, KIND, PS, GS, HS><<<(int)L.n_dir_targets, kP2PThreads, 0, st>>>(
       L.dir_tgt.ptr, L.dir_off.ptr, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
       stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13);
@@ -266,6 +269,7 @@ void run_direct(const double4* tpos, int64_t nt, const double4* spos, const doub
   constexpr int T = tpt<KIND>();
   int64_t blocks = (nt + kP2PThreads * T - 1) / (kP2PThreads * T);
   if (blocks == 0) return;
+  note_launch();
   k_direct<R, KIND, PS, GS, HS><<<(int)blocks, kP2PThreads, 0, st>>>(tpos, nt, spos, sstr, ns, acc13);
   FMM_CUDA_TRY(cudaGetLastError());
 }
@@ -314,7 +318,26 @@ struct DirectLaunch {
   }
 };
 
+__global__ void k_pair_count(const int* __restrict__ dt, const int* __restrict__ ds, int64_t n,
+                             const int* __restrict__ tcount, const int* __restrict__ scount,
+                             unsigned long long* __restrict__ out) {
+  unsigned long long v = 0;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    v += (unsigned long long)tcount[dt[k]] * (unsigned long long)scount[ds[k]];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, v);
+}
+
 }  // namespace
+
+void count_p2p_pairs(const DevTree& tt, const DevTree& stt, const DevLists& L, unsigned long long* out,
+                     cudaStream_t st) {
+  if (L.n_direct == 0) return;
+  int g = (int)std::min<int64_t>((L.n_direct + 255) / 256, 148 * 8);
+  note_launch();
+  k_pair_count<<<g, 256, 0, st>>>(L.dir_t.ptr, L.dir_s.ptr, L.n_direct, tt.body_count.ptr, stt.body_count.ptr, out);
+  FMM_CUDA_TRY(cudaGetLastError());
+}
 
 void launch_p2p(const DevTree& tt, const DevTree& stt, const DevLists& L, double* acc13, int kind, bool ps, bool gs,
                 bool hs, int precision, cudaStream_t st) {

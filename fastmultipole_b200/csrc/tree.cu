@@ -431,6 +431,7 @@ void unpack_bodies(DevTree& t, const double* dev_buf, int64_t n, int64_t stride,
   t.pos.grow(n);
   t.str.grow(n);
   if (n == 0) return;
+  note_launch();
   k_unpack<<<blocks_for(n), kThreads, 0, st>>>(dev_buf, n, stride, n_strength, has_radius ? 1 : 0, t.pos.ptr,
                                                t.str.ptr);
   FMM_CUDA_TRY(cudaGetLastError());
@@ -447,7 +448,9 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
   sc.tmp_d.grow(6 * (size_t)nb_part + 8);
   double* part = sc.tmp_d.ptr;
   RootGeom* root = reinterpret_cast<RootGeom*>(part + 6 * nb_part);
+  note_launch();
   k_bbox_partial<<<nb_part, kThreads, 0, st>>>(t.pos.ptr, n, part);
+  note_launch();
   k_bbox_final<<<1, 32, 0, st>>>(part, nb_part, root);
 
   // octant-path keys, sorted (stable) with the body index
@@ -455,6 +458,7 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
   sc.keys_b.grow(n);
   sc.vals_a.grow(n);
   sc.vals_b.grow(n);
+  note_launch();
   k_keys<<<blocks_for(n), kThreads, 0, st>>>(t.pos.ptr, n, root, sc.keys_a.ptr, sc.vals_a.ptr);
   size_t tmp_bytes = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, sc.keys_a.ptr, sc.keys_b.ptr, sc.vals_a.ptr, sc.vals_b.ptr,
@@ -484,6 +488,7 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
   sc.counts.grow(4);
   sc.flag.grow(1);
   FMM_CUDA_TRY(cudaMemsetAsync(sc.flag.ptr, 0, sizeof(int), st));
+  note_launch();
   k_root<<<1, 1, 0, st>>>(root, n, t.body_start.ptr, t.body_count.ptr, t.parent.ptr, t.level.ptr, t.gcenter.ptr,
                           t.gbox.ptr, t.gradius.ptr);
   FMM_CUDA_TRY(cudaGetLastError());
@@ -495,6 +500,7 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
     sc.tmp_i.grow(nl + 1);
     sc.tmp_j.grow(nl + 1);
     int g = (nl + 127) / 128;
+    note_launch();
     k_count_children<<<g, 128, 0, st>>>(keys, ls_node, le_node, level, leaf_size, method, t.body_start.ptr,
                                         t.body_count.ptr, sc.tmp_i.ptr, sc.flag.ptr);
     FMM_CUDA_TRY(cudaMemsetAsync(sc.tmp_i.ptr + nl, 0, sizeof(int), st));
@@ -510,6 +516,7 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
               "octree deeper than 21 levels: bodies are (nearly) coincident; spread them or raise leaf_size");
     int total = h[0];
     ensure((size_t)le_node + total + 1);
+    note_launch();
     k_emit_children<<<g, 128, 0, st>>>(keys, ls_node, le_node, level, sc.tmp_i.ptr, sc.tmp_j.ptr, t.body_start.ptr,
                                        t.body_count.ptr, t.child_start.ptr, t.n_children.ptr, t.parent.ptr,
                                        t.level.ptr, t.gcenter.ptr, t.gbox.ptr, t.gradius.ptr);
@@ -530,6 +537,7 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
   sc.tmp_i.grow(nb + 1);
   sc.tmp_j.grow(nb + 1);
   int gb = (nb + 255) / 256;
+  note_launch();
   k_leaf_flags<<<gb, 256, 0, st>>>(t.n_children.ptr, nb, sc.tmp_i.ptr);
   FMM_CUDA_TRY(cudaMemsetAsync(sc.tmp_i.ptr + nb, 0, sizeof(int), st));
   size_t sb = 0;
@@ -541,13 +549,16 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
   FMM_CUDA_TRY(cudaStreamSynchronize(st));
   t.n_leaves = nleaves;
   t.leaf_index.grow(nleaves);
+  note_launch();
   k_leaf_index<<<gb, 256, 0, st>>>(t.n_children.ptr, sc.tmp_j.ptr, nb, t.i_leaf.ptr, t.leaf_index.ptr);
 
   // final body order: by leaf (key order), input order inside each leaf
   unsigned int* key_in = reinterpret_cast<unsigned int*>(sc.keys_a.ptr);
   unsigned int* key_out = key_in + n;
+  note_launch();
   k_leaf_keys<<<(int)((nleaves * 32ll + 255) / 256), 256, 0, st>>>(t.leaf_index.ptr, nleaves, t.body_start.ptr,
                                                                     t.body_count.ptr, perm, key_in);
+  note_launch();
   k_iota<<<blocks_for(n), kThreads, 0, st>>>(sc.vals_a.ptr, n);
   t.sort_index.grow(n);
   int bits = 1;
@@ -564,6 +575,7 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
   double4* in_str = in_pos + n;
   FMM_CUDA_TRY(cudaMemcpyAsync(in_pos, t.pos.ptr, n * sizeof(double4), cudaMemcpyDeviceToDevice, st));
   FMM_CUDA_TRY(cudaMemcpyAsync(in_str, t.str.ptr, n * sizeof(double4), cudaMemcpyDeviceToDevice, st));
+  note_launch();
   k_permute<<<blocks_for(n), kThreads, 0, st>>>(in_pos, in_str, t.sort_index.ptr, n, t.pos.ptr, t.str.ptr);
 
   // branch geometry: shrink_recenter! (src/tree.jl:1176-1188) or the geometric cells
@@ -575,14 +587,17 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
   t.sbox.grow(3 * nb);
   t.max_influence.grow(nb);
   FMM_CUDA_TRY(cudaMemsetAsync(t.max_influence.ptr, 0, nb * sizeof(double), st));
+  note_launch();
   k_copy_geometry<<<gb, 256, 0, st>>>(nb, t.gcenter.ptr, t.gbox.ptr, t.gradius.ptr, t.tcenter.ptr, t.scenter.ptr,
                                       t.tradius.ptr, t.sradius.ptr, t.tbox.ptr, t.sbox.ptr);
   if (shrink) {
+    note_launch();
     k_shrink_leaves<<<(int)((nleaves * 32ll + 255) / 256), 256, 0, st>>>(
         t.leaf_index.ptr, nleaves, t.body_start.ptr, t.body_count.ptr, t.pos.ptr, t.tcenter.ptr, t.scenter.ptr,
         t.tradius.ptr, t.sradius.ptr, t.tbox.ptr, t.sbox.ptr);
     for (int l = t.n_levels - 1; l >= 0; --l) {
       int l0 = (int)t.levels_start[l], l1 = (int)t.levels_end[l];
+      note_launch();
       k_shrink_branches<<<(l1 - l0 + 127) / 128, 128, 0, st>>>(l0, l1, t.child_start.ptr, t.n_children.ptr,
                                                                t.tcenter.ptr, t.scenter.ptr, t.tradius.ptr,
                                                                t.sradius.ptr, t.tbox.ptr, t.sbox.ptr);
@@ -593,11 +608,13 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
 
 void branch_max_influence(DevTree& t, const double* out16_orig, cudaStream_t st) {
   int nl = (int)t.n_leaves;
+  note_launch();
   k_leaf_maxinf<<<(int)((nl * 32ll + 255) / 256), 256, 0, st>>>(t.leaf_index.ptr, nl, t.body_start.ptr,
                                                                 t.body_count.ptr, t.sort_index.ptr, out16_orig,
                                                                 t.max_influence.ptr);
   for (int l = t.n_levels - 1; l >= 0; --l) {
     int l0 = (int)t.levels_start[l], l1 = (int)t.levels_end[l];
+    note_launch();
     k_branch_maxinf<<<(l1 - l0 + 127) / 128, 128, 0, st>>>(l0, l1, t.child_start.ptr, t.n_children.ptr,
                                                            t.max_influence.ptr);
   }

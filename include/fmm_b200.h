@@ -120,6 +120,8 @@ typedef struct {
   int64_t m2l_flops;   /* algorithmic M2L flops at the orders actually used  */
   /* stage times on the device stream [ms]; zero unless timing was requested */
   double t_total_ms, t_tree_ms, t_lists_ms, t_nearfield_ms, t_upward_ms, t_horizontal_ms, t_downward_ms;
+  int64_t n_kernel_launches; /* kernels of this library launched by the solve (CUB sort/scan
+                                passes not included)                                       */
 } fmm_result;
 
 typedef struct fmm_ctx fmm_ctx;
