@@ -1,0 +1,202 @@
+"""
+    FastMultipoleB200
+
+Julia binding of libfmmb200.so (C ABI in include/fmm_b200.h) that keeps
+FastMultipole.jl's user API for the evaluation hot path: a user system overloads
+the same interface functions (`source_system_to_buffer!`, `data_per_body`,
+`get_position`, `strength_dims`, `get_n_bodies`, `body_to_multipole!`,
+`buffer_to_target_system!`, `has_vector_potential`) and calls `fmm!` / `direct!`
+with the reference's keyword arguments.  Gathering and scattering happen in
+Julia through those overloads; everything in between runs on the B200.
+
+Load it next to FastMultipole.jl (it reuses the reference's interface function
+names so existing overloads apply unchanged):
+
+    using FastMultipole
+    include("FastMultipoleB200.jl"); using .FastMultipoleB200
+    FastMultipoleB200.fmm!(system; expansion_order=10, leaf_size=64, multipole_acceptance=0.5)
+"""
+module FastMultipoleB200
+
+import FastMultipole
+import FastMultipole: source_system_to_buffer!, data_per_body, get_position, strength_dims, get_n_bodies,
+                      buffer_to_target_system!, has_vector_potential, DerivativesSwitch, Point, Source, Vortex,
+                      PowerAbsoluteGradient, PowerRelativeGradient, RotatedCoefficientsAbsoluteGradient,
+                      RotatedCoefficientsRelativeGradient, SelfTuningTreeStop, SelfTuning, Barba
+
+const libfmm = joinpath(@__DIR__, "..", "libfmmb200.so")
+
+# ---- C structs (field order and types of include/fmm_b200.h) ----
+struct FmmSourceSystem
+    kind::Cint
+    n_bodies::Int64
+    data_per_body::Cint
+    buffer::Ptr{Cdouble}
+    memory::Cint
+end
+
+struct FmmTargetSystem
+    n_bodies::Int64
+    positions::Ptr{Cdouble}
+    stride::Int64
+    out::Ptr{Cdouble}
+    memory::Cint
+end
+
+mutable struct FmmOptions
+    expansion_order::Cint
+    leaf_size_source::Cint
+    leaf_size_target::Cint
+    multipole_acceptance::Cdouble
+    error_method::Cint
+    error_tolerance::Cdouble
+    bonus_expansion::Cint
+    shrink_recenter::Cint
+    list_method::Cint
+    farfield::Cint
+    nearfield::Cint
+    self_induced::Cint
+    upward_pass::Cint
+    horizontal_pass::Cint
+    downward_pass::Cint
+    scalar_potential::Cint
+    gradient::Cint
+    hessian::Cint
+    precision::Cint
+end
+
+mutable struct FmmResult
+    p_max::Cint
+    error_success::Cint
+    n_target_branches::Int64
+    n_source_branches::Int64
+    n_target_leaves::Int64
+    n_source_leaves::Int64
+    n_m2l::Int64
+    n_direct::Int64
+    n_p2p_pairs::Int64
+    m2l_flops::Int64
+    t_total_ms::Cdouble
+    t_tree_ms::Cdouble
+    t_lists_ms::Cdouble
+    t_nearfield_ms::Cdouble
+    t_upward_ms::Cdouble
+    t_horizontal_ms::Cdouble
+    t_downward_ms::Cdouble
+    n_kernel_launches::Int64
+end
+FmmResult() = FmmResult(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
+
+const CTX = Ref{Ptr{Cvoid}}(C_NULL)
+
+function context()
+    if CTX[] == C_NULL
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        rc = ccall((:fmm_ctx_create, libfmm), Cint, (Ref{Ptr{Cvoid}}, Cint), h, 0)
+        rc == 0 || error("fmm_ctx_create failed with status $rc (no sm_100 GPU?)")
+        CTX[] = h[]
+    end
+    return CTX[]
+end
+
+function check(rc)
+    if rc != 0
+        msg = unsafe_string(ccall((:fmm_ctx_last_error, libfmm), Cstring, (Ptr{Cvoid},), context()))
+        error("libfmmb200 status $rc: $msg")
+    end
+end
+
+kernel_kind(system) = has_vector_potential(system) ? Cint(3) : Cint(1)
+
+error_code(::Nothing) = (Cint(0), 0.0, Cint(1))
+error_code(::PowerAbsoluteGradient{E,BE}) where {E,BE} = (Cint(1), Float64(E), Cint(BE))
+error_code(::PowerRelativeGradient{E,BE}) where {E,BE} = (Cint(2), Float64(E), Cint(BE))
+error_code(::RotatedCoefficientsAbsoluteGradient{E,BE}) where {E,BE} = (Cint(3), Float64(E), Cint(BE))
+error_code(::RotatedCoefficientsRelativeGradient{E,BE}) where {E,BE} = (Cint(4), Float64(E), Cint(BE))
+
+list_code(::SelfTuningTreeStop) = Cint(0)
+list_code(::Barba) = Cint(1)
+list_code(::SelfTuning) = Cint(2)
+
+# gather: source_system_to_buffer! in body order (src/compatibility.jl:377-387)
+function source_buffer(system)
+    n = get_n_bodies(system)
+    buf = zeros(Float64, data_per_body(system), n)
+    for i in 1:n
+        source_system_to_buffer!(buf, i, system, i)
+    end
+    return buf
+end
+
+# scatter: buffer_to_target_system! (src/compatibility.jl:324-338)
+function scatter!(system, out, switch)
+    for i in 1:get_n_bodies(system)
+        buffer_to_target_system!(system, i, switch, out, i)
+    end
+end
+
+"""
+    fmm!(target_system, source_system; kwargs...)
+    fmm!(system; leaf_size=20, kwargs...)
+
+FastMultipole.fmm! (src/fmm.jl:807-1176) on the B200.  Keyword arguments as the
+reference's; `precision=:mixed` selects the FP32 evaluation path.
+"""
+function fmm!(target_system, source_system; expansion_order=5, leaf_size_source=20, leaf_size_target=nothing,
+              multipole_acceptance=0.4, error_tolerance=nothing, shrink_recenter=true,
+              interaction_list_method=SelfTuningTreeStop(), scalar_potential=false, gradient=true, hessian=false,
+              farfield=true, nearfield=true, self_induced=true, upward_pass=true, horizontal_pass=true,
+              downward_pass=true, precision=:f64)
+    self_eval = target_system === source_system
+    buf = source_buffer(source_system)
+    n_s = size(buf, 2)
+    n_t = self_eval ? n_s : get_n_bodies(target_system)
+    pos = self_eval ? buf : reduce(hcat, [Vector{Float64}(get_position(target_system, i)) for i in 1:n_t])
+    out = zeros(Float64, 16, n_t)
+    em, eps, be = error_code(error_tolerance)
+    opt = FmmOptions(expansion_order, leaf_size_source, something(leaf_size_target, 0), multipole_acceptance,
+                     em, eps, be, shrink_recenter, list_code(interaction_list_method), farfield, nearfield,
+                     self_induced, upward_pass, horizontal_pass, downward_pass, scalar_potential, gradient, hessian,
+                     precision == :mixed ? 1 : 0)
+    res = FmmResult()
+    GC.@preserve buf pos out begin
+        src = FmmSourceSystem(kernel_kind(source_system), n_s, size(buf, 1), pointer(buf), 0)
+        tgt = FmmTargetSystem(n_t, self_eval ? Ptr{Cdouble}(C_NULL) : pointer(pos), 3, pointer(out), 0)
+        check(ccall((:fmm_solve, libfmm), Cint,
+                    (Ptr{Cvoid}, Ref{FmmTargetSystem}, Ref{FmmSourceSystem}, Ref{FmmOptions}, Ref{FmmResult}),
+                    context(), tgt, src, opt, res))
+    end
+    switch = DerivativesSwitch(scalar_potential, gradient, hessian)
+    scatter!(target_system, out, switch)
+    optimized_args = (leaf_size_source=leaf_size_source, expansion_order=max(expansion_order, 1),
+                      multipole_acceptance=multipole_acceptance)
+    return optimized_args, res, res.error_success != 0
+end
+
+fmm!(system; leaf_size=20, kwargs...) = fmm!(system, system; leaf_size_source=leaf_size, kwargs...)
+
+"""
+    direct!(target_system, source_system; scalar_potential=false, gradient=true, hessian=false)
+
+FastMultipole.direct! (src/direct.jl:20-75) on the B200, all pairs.
+"""
+function direct!(target_system, source_system; scalar_potential=false, gradient=true, hessian=false,
+                 precision=:f64)
+    buf = source_buffer(source_system)
+    n_t = get_n_bodies(target_system)
+    pos = reduce(hcat, [Vector{Float64}(get_position(target_system, i)) for i in 1:n_t])
+    out = zeros(Float64, 16, n_t)
+    GC.@preserve buf pos out begin
+        src = FmmSourceSystem(kernel_kind(source_system), size(buf, 2), size(buf, 1), pointer(buf), 0)
+        tgt = FmmTargetSystem(n_t, pointer(pos), 3, pointer(out), 0)
+        check(ccall((:fmm_direct, libfmm), Cint,
+                    (Ptr{Cvoid}, Ref{FmmTargetSystem}, Ref{FmmSourceSystem}, Cint, Cint, Cint, Cint),
+                    context(), tgt, src, scalar_potential, gradient, hessian, precision == :mixed ? 1 : 0))
+    end
+    scatter!(target_system, out, DerivativesSwitch(scalar_potential, gradient, hessian))
+    return nothing
+end
+
+direct!(system; kwargs...) = direct!(system, system; kwargs...)
+
+end # module
