@@ -83,6 +83,8 @@ SIGNATURES = {
                             C.POINTER(Result)]),
     "fmm_direct": (C.c_int, [C.c_void_p, C.POINTER(TargetSystem), C.POINTER(SourceSystem), C.c_int, C.c_int,
                              C.c_int, C.c_int]),
+    "fmm_direct_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.POINTER(TargetSystem), C.POINTER(SourceSystem), C.c_int,
+                                     C.c_int, C.c_int, C.c_int]),
     "fmm_get_tree": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TreeView)]),
     "fmm_get_lists": (C.c_int, [C.c_void_p, _i32p, _i64p, _i32p, _i64p]),
     "fmm_get_expansions": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int64]),

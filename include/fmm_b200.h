@@ -157,6 +157,24 @@ FMM_API int fmm_solve(fmm_ctx* ctx, const fmm_target_system* target, const fmm_s
 FMM_API int fmm_direct(fmm_ctx* ctx, const fmm_target_system* target, const fmm_source_system* source,
                int scalar_potential, int gradient, int hessian, int precision);
 
+/* ---- direct! without device allocations --------------------------------------
+ * No counterpart in the reference: an all-pairs direct! (same kernels as
+ * fmm_direct) for callers that cannot allocate device memory -- code running
+ * while a CUDA graph is captured, hosts that give the library a fixed
+ * device-memory arena, real-time loops that must not touch the allocator.
+ * Needs no context and allocates nothing: inputs and output must be device
+ * memory (FMM_MEMORY_DEVICE), and the only other memory used is a static
+ * 6.6 MB array that every GPU loading the library holds until exit.
+ * Limits: at most 32,768 sources and 32,768 targets (FMM_ERR_MEMORY beyond).
+ * The work is queued on `cuda_stream` (NULL = legacy default stream) and the
+ * call returns without synchronising; target->out is valid in stream order.
+ * The first call on a device looks up the array's device address, so make
+ * that first call before any stream capture.  Calls share the array: calls
+ * that overlap on the GPU (other streams or host threads) race on it. */
+FMM_API int fmm_direct_noalloc(int device, void* cuda_stream, const fmm_target_system* target,
+                               const fmm_source_system* source, int scalar_potential, int gradient, int hessian,
+                               int precision);
+
 /* ---- parity exports of the last fmm_solve (host memory) -------------------- */
 typedef struct {
   int64_t n_branches, n_levels, n_leaves, n_bodies;
