@@ -287,7 +287,8 @@ def gpu_arm(args, w, rank, world, local_rank):
     near_flops = st_mixed["n_p2p_pairs"] * w["flops_per_pair"]
     stages = {"nearfield": st_mixed["t_nearfield_ms"], "horizontal": st_mixed["t_horizontal_ms"],
               "upward": st_mixed["t_upward_ms"], "downward": st_mixed["t_downward_ms"],
-              "tree": st_mixed["t_tree_ms"], "lists": st_mixed["t_lists_ms"]}
+              "tree": st_mixed["t_tree_ms"], "lists": st_mixed["t_lists_ms"],
+              "influence_estimate": st_mixed["t_influence_ms"]}
     dom = max(("nearfield", "horizontal"), key=lambda k: stages[k])
     if dom == "nearfield":
         ach = near_flops / (stages["nearfield"] * 1e-3) / 1e12
@@ -318,7 +319,8 @@ def gpu_arm(args, w, rank, world, local_rank):
         "stages_ms": stages, "f64_stages_ms": {"nearfield": st_f64["t_nearfield_ms"],
                                                "horizontal": st_f64["t_horizontal_ms"],
                                                "upward": st_f64["t_upward_ms"], "downward": st_f64["t_downward_ms"],
-                                               "tree": st_f64["t_tree_ms"], "lists": st_f64["t_lists_ms"]},
+                                               "tree": st_f64["t_tree_ms"], "lists": st_f64["t_lists_ms"],
+                                               "influence_estimate": st_f64["t_influence_ms"]},
         "p_max": st_mixed["p_max"], "n_m2l": st_mixed["n_m2l"], "n_direct": st_mixed["n_direct"],
         "n_p2p_pairs": st_mixed["n_p2p_pairs"],
         "roofline": roof,

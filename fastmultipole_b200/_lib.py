@@ -57,7 +57,8 @@ class Result(C.Structure):
                 ("m2l_flops", C.c_int64),
                 ("t_total_ms", C.c_double), ("t_tree_ms", C.c_double), ("t_lists_ms", C.c_double),
                 ("t_nearfield_ms", C.c_double), ("t_upward_ms", C.c_double), ("t_horizontal_ms", C.c_double),
-                ("t_downward_ms", C.c_double), ("n_kernel_launches", C.c_int64)]
+                ("t_downward_ms", C.c_double), ("n_kernel_launches", C.c_int64),
+                ("t_influence_ms", C.c_double)]
 
 
 class TreeView(C.Structure):

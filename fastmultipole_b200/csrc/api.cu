@@ -202,7 +202,8 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
       float ms[7];
       for (int k = 0; k < 7; ++k) FMM_CUDA_TRY(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
       res->t_tree_ms = ms[0];
-      res->t_lists_ms = ms[1] + ms[2];
+      res->t_lists_ms = ms[1];
+      res->t_influence_ms = ms[2];
       res->t_nearfield_ms = ms[3];
       res->t_upward_ms = ms[4];
       res->t_horizontal_ms = ms[5];

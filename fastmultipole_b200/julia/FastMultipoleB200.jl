@@ -84,8 +84,9 @@ mutable struct FmmResult
     t_horizontal_ms::Cdouble
     t_downward_ms::Cdouble
     n_kernel_launches::Int64
+    t_influence_ms::Cdouble
 end
-FmmResult() = FmmResult(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
+FmmResult() = FmmResult(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
 
 const CTX = Ref{Ptr{Cvoid}}(C_NULL)
 

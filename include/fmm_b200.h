@@ -122,6 +122,7 @@ typedef struct {
   double t_total_ms, t_tree_ms, t_lists_ms, t_nearfield_ms, t_upward_ms, t_horizontal_ms, t_downward_ms;
   int64_t n_kernel_launches; /* kernels of this library launched by the solve (CUB sort/scan
                                 passes not included)                                       */
+  double t_influence_ms;       /* influence estimate of the relative error methods [ms]    */
 } fmm_result;
 
 typedef struct fmm_ctx fmm_ctx;
