@@ -99,6 +99,9 @@ void launch_p2m(DevTree& s, int p, int kind, const DevTables& tb, cudaStream_t s
 void launch_m2m(DevTree& s, int p, bool lh, const DevTables& tb, cudaStream_t st);
 // per-pair orders go to p_used (device, one per m2l entry) when non-null; stats (device,
 // 4 ints, zeroed by the caller) receives the max order, a failure flag and the flop count
+// lane-per-pair M2L (m2l_lane.cu): point sources, orders 1..12; false = not handled
+bool launch_m2l_lane(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh, int em, double eps, int be,
+                     int* p_used, int* stats, cudaStream_t st);
 void launch_m2l(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh, int error_method, double eps,
                 int be, int* p_used, int* stats, const DevTables& tb, cudaStream_t st);
 void launch_l2l(DevTree& t, int p, bool lh, const DevTables& tb, cudaStream_t st);

@@ -17,6 +17,7 @@
 // Expansion layout: 4*Nh doubles per branch, e[4*i + 2*set + reim], i = n(n+1)/2 + m,
 // set 0 = phi, set 1 = chi (Lamb-Helmholtz), as the reference's Tree.expansions.
 #include "engine.cuh"
+#include "pair_m2l.cuh"
 
 namespace fmmb {
 
@@ -121,6 +122,47 @@ __global__ void __launch_bounds__(32 * kWarps) k_m2l(const int* __restrict__ tgt
     atomicMax(stats.pmax, pmax);
     if (!all_ok) atomicExch(stats.fail, 1);
     atomicAdd(stats.flops, fl);
+  }
+}
+
+// M2L at orders <= 3 without error control: warp per target, lane per pair
+// (thread-per-pair chain of pair_m2l.cuh), lane partials summed by shuffles
+template <int P, bool LH>
+__global__ void __launch_bounds__(32 * kWarps) k_m2l_pair(const int* __restrict__ tgt_list,
+                                                          const int* __restrict__ off, const int* __restrict__ src_of,
+                                                          int n_targets, double* __restrict__ local,
+                                                          const double* __restrict__ multipole,
+                                                          const double* __restrict__ tcen,
+                                                          const double* __restrict__ scen, int* __restrict__ p_used,
+                                                          Tab tb, M2LStats stats) {
+  using K = eng::PairM2L<P, LH>;
+  constexpr int NV = K::NH * K::NC;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int b = blockIdx.x * kWarps + wid;
+  if (b >= n_targets) return;
+  const int t = tgt_list[b];
+  const int64_t NH4 = 4 * K::NH;
+  const double tx = tcen[3 * t], ty = tcen[3 * t + 1], tz = tcen[3 * t + 2];
+  double acc[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+  const int l0 = off[b], l1 = off[b + 1];
+  for (int l = l0 + lane; l < l1; l += 32) {
+    const int s = src_of[l];
+    K::run(acc, multipole + NH4 * s, tx - scen[3 * s], ty - scen[3 * s + 1], tz - scen[3 * s + 2], tb);
+    if (p_used) p_used[l] = P;
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
+  double* dst = local + NH4 * t;
+#pragma unroll
+  for (int v = 0; v < NV; ++v)
+    if ((v & 31) == lane) dst[4 * (v / K::NC) + (v % K::NC)] += acc[v];
+  if (lane == 0) {
+    atomicMax(stats.pmax, P);
+    atomicAdd(stats.flops, (unsigned long long)(l1 - l0) * m2l_pair_flops(P, LH));
   }
 }
 
@@ -816,6 +858,27 @@ void launch_m2l(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh,
   if (L.n_m2l_targets == 0) return;
   // stats: [0] = max order used, [1] = any tolerance missed, [2..3] = flop count (u64)
   M2LStats S{stats, stats + 1, reinterpret_cast<unsigned long long*>(stats + 2)};
+  if (em == FMM_ERROR_NONE && p >= 1 && p <= 3) {
+    int g = (int)((L.n_m2l_targets + kWarps - 1) / kWarps);
+    Tab T = tab_of(tb);
+    note_launch();
+#define FMM_M2L_PAIR(PP, LL)                                                                                   \
+  k_m2l_pair<PP, LL><<<g, 32 * kWarps, 0, st>>>(L.m2l_tgt.ptr, L.m2l_off.ptr, L.m2l_s.ptr, (int)L.n_m2l_targets, \
+                                                t.local.ptr, s.multipole.ptr, t.tcenter.ptr, s.scenter.ptr, p_used, T, S)
+    if (lh) {
+      if (p == 1) FMM_M2L_PAIR(1, true);
+      else if (p == 2) FMM_M2L_PAIR(2, true);
+      else FMM_M2L_PAIR(3, true);
+    } else {
+      if (p == 1) FMM_M2L_PAIR(1, false);
+      else if (p == 2) FMM_M2L_PAIR(2, false);
+      else FMM_M2L_PAIR(3, false);
+    }
+#undef FMM_M2L_PAIR
+    FMM_CUDA_TRY(cudaGetLastError());
+    return;
+  }
+  if (launch_m2l_lane(t, s, L, p, lh, em, eps, be, p_used, stats, st)) return;
   M2LLaunch f{t, s, L, p, em, be, eps, p_used, S, tab_of(tb), st};
   dispatch_slots(p, lh, f);
 }

@@ -1,0 +1,555 @@
+// m2l_lane.cu -- lane-per-pair M2L for point sources, orders 1..kLaneMaxP,
+// plain and error-controlled.
+//
+// One warp owns one target branch and takes its M2L sources 32 at a time, one
+// (target, source) pair per lane.  Each lane runs the reference's chain
+// (multipole_to_local!, src/translate.jl:519-550 and :555-829, :1124-1412):
+// rotate_z -> rotate_y -> [degree-by-degree error control] -> coaxial
+// translation -> rotate_y back -> back_rotate_z, and the 32 results of every
+// degree are summed across the lanes into the warp's accumulator.
+//
+// Rotation about y.  The reference builds the Wigner matrix of each degree at
+// beta for every pair (update_Ts_n!, src/rotate.jl:363-441),
+//   T(m', m) = sum_nu w_nu H(m', nu) H(m, nu) Re(i^(m + |m'|) e^{i nu beta})  (x (-1)^(n+nu) for m' <= 0),
+// H the Wigner matrix at pi/2, w_0 = 1, w_nu>0 = 2, and applies it with the
+// magnitudes mag(m, a) = A(m) B(a) (src/rotate.jl:660-689, :975-1004) and the
+// phases i^(a - m).  Substituting T and splitting the input by the parity of a
+// gives, for the multipole (local: e^{+-i nu beta} exchanged),
+//   E_nu = sum_{a even >= 2} B(a) H(a, nu) X(a),  O_nu = sum_{a odd} B(a) H(a, nu) X(a),
+//   Z_nu = B(0) H(0, nu) X(0),
+//   S1 = E - O,  S3 = E + O,  S2 = conj(Z + E + O),  S4 = conj(Z + E - O),  s = (-1)^(n + nu),
+//   P_nu = e^{i nu beta} (S1 + s S2),  Q_nu = e^{-i nu beta} (S3 + s S4),
+//   out(m) = sum_nu [A(m) H(m, nu) w_nu / 2] (P_nu + (-1)^m Q_nu),
+// two products with constant (n+1) x (n+1) matrices per degree instead of a
+// per-pair O(n^3) matrix build and an O(n^2) application.  The constant
+// matrices B H and A H w / 2 of both magnitude sets live in constant memory;
+// every degree is a compile-time specialisation, so the expansions of a degree
+// sit in registers and the matrix entries are constant-bank operands.  The
+// rotated multipole of all degrees (needed by the coaxial step) is kept in the
+// warp's shared memory, one column per lane.
+#include <mutex>
+
+#include "context.cuh"
+
+namespace fmmb {
+
+namespace {
+
+constexpr int kLaneMaxP = 12;
+constexpr int kLenT = (kLaneMaxP + 1) * (kLaneMaxP + 2) * (2 * kLaneMaxP + 3) / 6;  // sum_n (n+1)^2
+constexpr int kNhMax = (kLaneMaxP + 1) * (kLaneMaxP + 2) / 2;
+constexpr unsigned kAll = 0xffffffffu;
+
+// [lenT(n-1) + row (n+1) + nu]: zeta (multipole) and eta (local) magnitude sets
+__constant__ double c_HBz[kLenT], c_HAz[kLenT], c_HBe[kLenT], c_HAe[kLenT];
+__constant__ double c_Mt[kNhMax], c_Lt[kNhMax];
+
+__host__ __device__ constexpr int hi(int n, int m) { return n * (n + 1) / 2 + m; }
+__host__ __device__ constexpr int lenT(int n) { return n < 0 ? 0 : (n + 1) * (n + 2) * (2 * n + 3) / 6; }
+
+template <bool LOCAL>
+__device__ __forceinline__ double HB(int n, int a, int nu) {
+  if constexpr (LOCAL)
+    return c_HBe[lenT(n - 1) + a * (n + 1) + nu];
+  else
+    return c_HBz[lenT(n - 1) + a * (n + 1) + nu];
+}
+template <bool LOCAL>
+__device__ __forceinline__ double HA(int n, int m, int nu) {
+  if constexpr (LOCAL)
+    return c_HAe[lenT(n - 1) + m * (n + 1) + nu];
+  else
+    return c_HAz[lenT(n - 1) + m * (n + 1) + nu];
+}
+
+std::mutex g_tab_mu;
+bool g_tab_done[64];
+
+// B H and A H w / 2 of both magnitude sets, degrees 0..kLaneMaxP, once per device
+void ensure_lane_tables(cudaStream_t st) {
+  int dev = 0;
+  FMM_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_tab_mu);
+  if (dev < 64 && g_tab_done[dev]) return;
+  HostTables h;
+  build_tables(h, kLaneMaxP);
+  std::vector<double> hbz(kLenT), haz(kLenT), hbe(kLenT), hae(kLenT), mt(kNhMax), lt(kNhMax);
+  for (int n = 0; n <= kLaneMaxP; ++n) {
+    const double* H = h.Hs.data() + length_Hs(n - 1);
+    const double* z = h.zeta.data() + length_Ts(n - 1);
+    const double* e = h.eta.data() + length_Ts(n - 1);
+    const int off = lenT(n - 1);
+    for (int a = 0; a <= n; ++a)
+      for (int nu = 0; nu <= n; ++nu) {
+        const double Hv = H[H_index(std::min(a, nu), std::max(a, nu))];
+        const double w = nu == 0 ? 0.5 : 1.0;
+        hbz[off + a * (n + 1) + nu] = z[a] * Hv;  // B(a): row 0 of the magnitudes
+        hbe[off + a * (n + 1) + nu] = e[a] * Hv;
+        haz[off + a * (n + 1) + nu] = z[a * (n + 1)] * Hv * w;  // A(m): column 0
+        hae[off + a * (n + 1) + nu] = e[a * (n + 1)] * Hv * w;
+      }
+  }
+  for (int i = 0; i < kNhMax; ++i) {
+    mt[i] = h.Mt[i];
+    lt[i] = h.Lt[i];
+  }
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBz, hbz.data(), kLenT * 8, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAz, haz.data(), kLenT * 8, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBe, hbe.data(), kLenT * 8, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAe, hae.data(), kLenT * 8, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Mt, mt.data(), kNhMax * 8, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Lt, lt.data(), kNhMax * 8, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaStreamSynchronize(st));
+  if (dev < 64) g_tab_done[dev] = true;
+}
+
+// rotate_y of degree N (X -> Y); LOCAL: eta set and e^{-+i nu beta}
+template <int N, bool LOCAL>
+__device__ __forceinline__ void rot_y_deg(const double (&Xr)[N + 1], const double (&Xi)[N + 1], double cb,
+                                          double sb, double (&Yr)[N + 1], double (&Yi)[N + 1]) {
+  double Rpr[N + 1], Rpi[N + 1], Rmr[N + 1], Rmi[N + 1];
+  double c = 1.0, s = 0.0;  // cos, sin (nu beta) by the reference's recurrence
+#pragma unroll
+  for (int nu = 0; nu <= N; ++nu) {
+    if (nu > 0) {
+      const double cn = cb * c - sb * s;
+      const double sn = sb * c + cb * s;
+      c = cn;
+      s = sn;
+    }
+    double Er = 0, Ei = 0, Or = 0, Oi = 0;
+#pragma unroll
+    for (int a = 1; a <= N; ++a) {
+      const double h = HB<LOCAL>(N, a, nu);
+      if (a & 1) {
+        Or += h * Xr[a];
+        Oi += h * Xi[a];
+      } else {
+        Er += h * Xr[a];
+        Ei += h * Xi[a];
+      }
+    }
+    const double h0 = HB<LOCAL>(N, 0, nu);
+    const double Zr = h0 * Xr[0], Zi = h0 * Xi[0];
+    const double sg = ((N + nu) & 1) ? -1.0 : 1.0;
+    const double S1r = Er - Or, S1i = Ei - Oi;
+    const double S3r = Er + Or, S3i = Ei + Oi;
+    const double S2r = Zr + S3r, S2i = -(Zi + S3i);
+    const double S4r = Zr + S1r, S4i = -(Zi + S1i);
+    const double A1r = S1r + sg * S2r, A1i = S1i + sg * S2i;
+    const double A3r = S3r + sg * S4r, A3i = S3i + sg * S4i;
+    const double ss = LOCAL ? -s : s;
+    const double Pr = c * A1r - ss * A1i, Pi = c * A1i + ss * A1r;
+    const double Qr = c * A3r + ss * A3i, Qi = c * A3i - ss * A3r;
+    Rpr[nu] = Pr + Qr;
+    Rpi[nu] = Pi + Qi;
+    Rmr[nu] = Pr - Qr;
+    Rmi[nu] = Pi - Qi;
+  }
+#pragma unroll
+  for (int m = 0; m <= N; ++m) {
+    double vr = 0, vi = 0;
+#pragma unroll
+    for (int nu = 0; nu <= N; ++nu) {
+      const double h = HA<LOCAL>(N, m, nu);
+      vr += h * ((m & 1) ? Rmr[nu] : Rpr[nu]);
+      vi += h * ((m & 1) ? Rmi[nu] : Rpi[nu]);
+    }
+    Yr[m] = vr;
+    Yi[m] = vi;
+  }
+}
+
+// per-lane state of one (target, source) pair
+struct Pair {
+  const double* src;  // multipole of the source branch (interleaved e[4 i + 2 set + reim])
+  double cph, sph, cth, sth, r, rinv;
+  int P;        // order used
+  bool valid;   // lane holds a pair
+  bool active;  // still inside the error-control loop
+  bool ok;      // tolerance met
+  // error control (src/translate.jl:1124-1412, :555-829)
+  double thr, r_mp_inv, r_mp_inv_np2, r_l, r_l_nm1, nm1_fact_inv, np1_fact, n_fact_t_np1, mp_phi, Mn0;
+};
+
+// rotated multipole in shared memory: plane c (re, im) of coefficient i, column lane
+__device__ __forceinline__ double& MS(double* Ms, int i, int c, int lane) { return Ms[(2 * i + c) * 32 + lane]; }
+
+// rotate_z + rotate_y of degree N of the lane's multipole into shared memory;
+// returns the multipole power of degree N (rotate_z_n_power!, weight 1 for every m)
+template <int N>
+__device__ __forceinline__ double fwd_degree(const Pair& q, double* Ms, int lane, double& y0r, double& y1r,
+                                             double& y1i) {
+  double Xr[N + 1], Xi[N + 1];
+  double er = 1.0, ei = 0.0, pw = 0.0;
+#pragma unroll
+  for (int a = 0; a <= N; ++a) {
+    const double2 u = __ldg(reinterpret_cast<const double2*>(q.src) + 2 * hi(N, a));
+    const double Nt = c_Mt[hi(N, a)];
+    pw += (u.x * u.x + u.y * u.y) * Nt * Nt;
+    Xr[a] = N == 0 ? u.x : u.x * er - u.y * ei;
+    Xi[a] = N == 0 ? u.y : u.x * ei + u.y * er;
+    const double t = er;
+    er = er * q.cph - ei * q.sph;
+    ei = t * q.sph + ei * q.cph;
+  }
+  double Yr[N + 1], Yi[N + 1];
+  rot_y_deg<N, false>(Xr, Xi, q.cth, q.sth, Yr, Yi);
+#pragma unroll
+  for (int m = 0; m <= N; ++m) {
+    MS(Ms, hi(N, m), 0, lane) = Yr[m];
+    MS(Ms, hi(N, m), 1, lane) = Yi[m];
+  }
+  y0r = Yr[0];
+  y1r = N >= 1 ? Yr[N >= 1 ? 1 : 0] : 0.0;
+  y1i = N >= 1 ? Yi[N >= 1 ? 1 : 0] : 0.0;
+  return sqrt(pw);
+}
+
+// (n + m)! / t^(n + m + 1) by the reference's recurrence (src/translate.jl:184-225)
+__device__ __forceinline__ double coef0(int n, int m, double one_over_t) {
+  double c = one_over_t;
+  for (int k = 0; k < n; ++k) c *= (k + 1) * one_over_t;
+  int nm = n;
+  for (int j = 0; j < m; ++j) {
+    nm += 1;
+    c *= nm * one_over_t;
+  }
+  return c;
+}
+
+// local error estimate of degree N from the rotated multipole of degrees <= N
+template <int N>
+__device__ __forceinline__ double eps_local(const Pair& q, const double* Ms, int lane, bool power) {
+  if (power) {
+    // degree N of translate_multipole_to_local_z_n! and local_power (src/translate.jl:238-295, :455-502)
+    double a = 0.0;
+#pragma unroll
+    for (int m = 0; m <= N; ++m) {
+      double c = coef0(N, m, q.rinv);
+      int n_np = N + m;
+      double vr = 0, vi = 0;
+#pragma unroll
+      for (int np = m; np <= N; ++np) {
+        vr += c * Ms[(2 * hi(np, m)) * 32 + lane];
+        vi += c * Ms[(2 * hi(np, m) + 1) * 32 + lane];
+        n_np += 1;
+        c *= n_np * q.rinv;
+      }
+      const double Nt = c_Lt[hi(N, m)];
+      a += (vr * vr + vi * vi) * Nt * Nt;
+    }
+    const double lphi = sqrt(a);
+    return 1.7320508075688772 * lphi * q.r_l_nm1 * q.nm1_fact_inv / c_Lt[hi(N, 0)];
+  }
+  // translate_multipole_to_local_z_m01_n (src/translate.jl:302-364)
+  double c = q.n_fact_t_np1;
+  int n_np = N;
+  double a0 = 0;
+#pragma unroll
+  for (int np = 0; np <= N; ++np) {
+    a0 += c * Ms[(2 * hi(np, 0)) * 32 + lane];
+    n_np += 1;
+    c *= n_np * q.rinv;
+  }
+  c = q.n_fact_t_np1 * ((N + 1) * q.rinv);
+  n_np = N + 1;
+  double b1r = 0, b1i = 0;
+#pragma unroll
+  for (int np = 1; np <= N; ++np) {
+    b1r += c * Ms[(2 * hi(np, 1)) * 32 + lane];
+    b1i += c * Ms[(2 * hi(np, 1) + 1) * 32 + lane];
+    n_np += 1;
+    c *= n_np * q.rinv;
+  }
+  return (fabs(b1r) + fabs(b1i) + fabs(a0)) * q.r_l_nm1 * q.nm1_fact_inv;
+}
+
+// error-controlled degrees N..PMAX: the reference's degree loop, one degree per
+// specialisation, until every lane has met its tolerance or PMAX is reached
+template <int N, int PMAX>
+__device__ __forceinline__ void err_loop(Pair& q, double* Ms, int lane, bool power, int be) {
+  if constexpr (N <= PMAX) {
+    if (!__any_sync(kAll, q.active)) return;
+    if (q.active) {
+      double y0r, y1r, y1i;
+      const double pn_phi = fwd_degree<N>(q, Ms, lane, y0r, y1r, y1i);
+      const double Mn0_next = c_Mt[hi(N, 0)];
+      double eps_mp;
+      if (power)
+        eps_mp = 1.7320508075688772 * q.mp_phi * q.r_mp_inv_np2 * q.np1_fact / q.Mn0;
+      else
+        eps_mp = (sqrt(y1r * y1r + y1i * y1i) + fabs(y0r)) * q.np1_fact * q.r_mp_inv_np2;
+      if (eps_mp <= q.thr) {
+        const double eps_l = eps_local<N>(q, Ms, lane, power);
+        if (eps_mp + eps_l * 2.0 <= q.thr) {
+          q.P = N - 1 + (be ? 1 : 0);
+          q.ok = true;
+          q.active = false;
+        }
+      }
+      if (q.active) {
+        if (power || N < PMAX) {
+          q.n_fact_t_np1 *= (N + 1) * q.rinv;
+          q.r_l_nm1 *= q.r_l;
+          q.r_mp_inv_np2 *= q.r_mp_inv;
+          q.nm1_fact_inv /= N;
+          q.np1_fact *= N + 1;
+        }
+        if (power) {
+          q.mp_phi = pn_phi;
+          q.Mn0 = Mn0_next;
+        }
+      }
+    }
+    err_loop<N + 1, PMAX>(q, Ms, lane, power, be);
+  }
+}
+
+// all degrees N..PMAX without error control
+template <int N, int PMAX>
+__device__ __forceinline__ void plain_loop(const Pair& q, double* Ms, int lane) {
+  if constexpr (N <= PMAX) {
+    if (q.valid) {
+      double y0r, y1r, y1i;
+      fwd_degree<N>(q, Ms, lane, y0r, y1r, y1i);
+    }
+    plain_loop<N + 1, PMAX>(q, Ms, lane);
+  }
+}
+
+// degree N of the local expansion: coaxial translation of the rotated multipole
+// (sources m..P), rotate_y back, back_rotate_z, then the sum over the 32 lanes
+// into the warp accumulator (stage: 2 (PMAX+1) rows of 33 doubles)
+template <int N, int PMAX>
+__device__ __forceinline__ void back_loop(const Pair& q, const double* Ms, double* stage, double* acc, int lane,
+                                          int pwarp) {
+  if constexpr (N <= PMAX) {
+    if (N > pwarp) return;
+    const bool on = q.valid && N <= q.P;
+    double Xr[N + 1], Xi[N + 1];
+#pragma unroll
+    for (int m = 0; m <= N; ++m) {
+      double c = coef0(N, m, q.rinv);
+      int n_np = N + m;
+      double vr = 0, vi = 0;
+#pragma unroll
+      for (int np = m; np <= PMAX; ++np) {
+        if (np <= q.P) {
+          vr += c * Ms[(2 * hi(np, m)) * 32 + lane];
+          vi += c * Ms[(2 * hi(np, m) + 1) * 32 + lane];
+        }
+        n_np += 1;
+        c *= n_np * q.rinv;
+      }
+      Xr[m] = on ? vr : 0.0;
+      Xi[m] = on ? vi : 0.0;
+    }
+    double Yr[N + 1], Yi[N + 1];
+    rot_y_deg<N, true>(Xr, Xi, q.cth, q.sth, Yr, Yi);
+    double er = 1.0, ei = 0.0;
+#pragma unroll
+    for (int m = 0; m <= N; ++m) {
+      const double cr = er, ci = -ei;
+      const double vr = N == 0 ? Yr[m] : Yr[m] * cr - Yi[m] * ci;
+      const double vi = N == 0 ? Yi[m] : Yr[m] * ci + Yi[m] * cr;
+      stage[(2 * m) * 33 + lane] = on ? vr : 0.0;
+      stage[(2 * m + 1) * 33 + lane] = on ? vi : 0.0;
+      const double t = er;
+      er = er * q.cph - ei * q.sph;
+      ei = t * q.sph + ei * q.cph;
+    }
+    __syncwarp();
+    if (lane < 2 * (N + 1)) {
+      double v = 0.0;
+#pragma unroll 8
+      for (int k = 0; k < 32; ++k) v += stage[lane * 33 + k];
+      acc[2 * hi(N, 0) + lane] += v;
+    }
+    __syncwarp();
+    back_loop<N + 1, PMAX>(q, Ms, stage, acc, lane, pwarp);
+  }
+}
+
+__device__ __forceinline__ unsigned long long lane_pair_flops(int P) {
+  // the reference's operation count: 4 [2 sum_n (n+1)(2n+1) + sum_n sum_m (P-m+1)]
+  unsigned long long rot = 0, coax = 0;
+  for (int n = 0; n <= P; ++n) {
+    rot += (unsigned long long)(n + 1) * (2 * n + 1);
+    for (int m = 0; m <= n; ++m) coax += (unsigned long long)(P - m + 1);
+  }
+  return 4ull * (2 * rot + coax);
+}
+
+// minimum_distance, src/error.jl:5-20
+__device__ __forceinline__ double minabs(double x, double y) {
+  return x * (fabs(x) <= fabs(y) ? 1.0 : 0.0) + y * (fabs(y) < fabs(x) ? 1.0 : 0.0);
+}
+__device__ __forceinline__ double min_dist_1d(double dx, double rm, double rp) {
+  double right = dx + rp, left = dx + rm;
+  double same = (right * left >= 0) ? 1.0 : 0.0;
+  return same * minabs(right, left);
+}
+
+template <int PMAX>
+__host__ __device__ constexpr size_t lane_smem_doubles() {
+  return (size_t)2 * hi(PMAX + 1, 0) * 32 + (size_t)2 * (PMAX + 1) * 33 + (size_t)2 * hi(PMAX + 1, 0);
+}
+
+// one warp per CTA; warp b owns target tgt_list[b] and its sources src_of[off[b] .. off[b+1])
+template <int PMAX>
+__global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_list, const int* __restrict__ off,
+                                                 const int* __restrict__ src_of, double* __restrict__ local,
+                                                 const double* __restrict__ multipole,
+                                                 const double* __restrict__ tcen, const double* __restrict__ tbox,
+                                                 const double* __restrict__ trad, const double* __restrict__ maxinf,
+                                                 const double* __restrict__ scen, int em, double eps_in, int be,
+                                                 int* __restrict__ p_used, int* __restrict__ st_pmax,
+                                                 int* __restrict__ st_fail,
+                                                 unsigned long long* __restrict__ st_flops) {
+  constexpr int NH = hi(PMAX + 1, 0);
+  extern __shared__ double lane_smem[];
+  double* Ms = lane_smem;                            // [2 NH][32]
+  double* stage = Ms + 2 * NH * 32;                  // [2 (PMAX+1)][33]
+  double* acc = stage + 2 * (PMAX + 1) * 33;         // [2 NH]
+  const int lane = threadIdx.x;
+  const int b = blockIdx.x;
+  const int t = tgt_list[b];
+  const double tc0 = tcen[3 * t], tc1 = tcen[3 * t + 1], tc2 = tcen[3 * t + 2];
+  const bool errc = em != FMM_ERROR_NONE;
+  const bool relative = (em == FMM_POWER_RELATIVE_GRADIENT || em == FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT);
+  const bool power = (em == FMM_POWER_ABSOLUTE_GRADIENT || em == FMM_POWER_RELATIVE_GRADIENT);
+  const double eps = relative ? maxinf[t] * eps_in : eps_in;
+  const double tb0 = tbox[3 * t], tb1 = tbox[3 * t + 1], tb2 = tbox[3 * t + 2];
+  const double r_l = trad[t];
+  for (int i = lane; i < 2 * NH; i += 32) acc[i] = 0.0;
+  int pmax = 0;
+  bool fail = false;
+  unsigned long long fl = 0;
+  const int l0 = off[b], l1 = off[b + 1];
+  for (int lb = l0; lb < l1; lb += 32) {
+    Pair q;
+    const int l = lb + lane;
+    q.valid = l < l1;
+    q.P = PMAX;
+    q.ok = true;
+    q.active = false;
+    q.src = multipole;
+    q.cph = 1.0;
+    q.sph = 0.0;
+    q.cth = 1.0;
+    q.sth = 0.0;
+    q.r = 1.0;
+    q.rinv = 1.0;
+    if (q.valid) {
+      const int s = src_of[l];
+      q.src = multipole + (int64_t)4 * NH * s;
+      const double x = tc0 - scen[3 * s], y = tc1 - scen[3 * s + 1], z = tc2 - scen[3 * s + 2];
+      // cartesian_to_spherical (src/rotate.jl:9-21) in cos/sin form
+      const double x2y2 = x * x + y * y;
+      const double r2 = x2y2 + z * z;
+      q.r = (r2 == 0.0) ? r2 : sqrt(r2);
+      if (x2y2 > 0) {
+        const double rho = sqrt(x2y2);
+        q.cph = x / rho;
+        q.sph = y / rho;
+        q.cth = z / q.r;
+        q.sth = rho / q.r;
+      } else {
+        q.cth = (q.r > 0 && z < 0) ? -1.0 : 1.0;
+      }
+      q.rinv = 1 / q.r;
+      if (errc) {
+        const double mdx = min_dist_1d(x, -tb0, tb0), mdy = min_dist_1d(y, -tb1, tb1), mdz = min_dist_1d(z, -tb2, tb2);
+        const double r_mp = sqrt(mdx * mdx + mdy * mdy + mdz * mdz);
+        q.r_mp_inv = 1.0 / r_mp;
+        q.r_mp_inv_np2 = q.r_mp_inv * q.r_mp_inv * q.r_mp_inv;
+        q.r_l = r_l;
+        q.r_l_nm1 = 1.0;
+        q.n_fact_t_np1 = q.rinv * q.rinv;
+        q.nm1_fact_inv = 1.0;
+        q.np1_fact = 2.0;
+        q.Mn0 = c_Mt[0];
+        q.mp_phi = sqrt((q.src[0] * q.src[0] + q.src[1] * q.src[1]) * q.Mn0 * q.Mn0);
+        q.thr = eps * 4 * kPi;
+        q.ok = false;
+        q.active = true;
+      }
+    }
+    if (errc) {
+      if (q.valid) {
+        double y0r, y1r, y1i;
+        fwd_degree<0>(q, Ms, lane, y0r, y1r, y1i);
+      }
+      err_loop<1, PMAX>(q, Ms, lane, power, be);
+      if (q.active) q.active = false;  // PMAX reached: P = PMAX, tolerance missed
+    } else {
+      plain_loop<0, PMAX>(q, Ms, lane);
+    }
+    int pw = q.valid ? q.P : -1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) pw = max(pw, __shfl_xor_sync(kAll, pw, o));
+    __syncwarp();
+    back_loop<0, PMAX>(q, Ms, stage, acc, lane, pw);
+    if (q.valid) {
+      if (p_used) p_used[l] = q.P;
+      pmax = max(pmax, q.P);
+      fail = fail || !q.ok;
+      fl += lane_pair_flops(q.P);
+    }
+    __syncwarp();
+  }
+  double* dst = local + (int64_t)4 * NH * t;
+  for (int i = lane; i < 2 * NH; i += 32) dst[4 * (i >> 1) + (i & 1)] += acc[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    pmax = max(pmax, __shfl_xor_sync(kAll, pmax, o));
+    fl += __shfl_xor_sync(kAll, fl, o);
+  }
+  const bool any_fail = __any_sync(kAll, fail);
+  if (lane == 0) {
+    atomicMax(st_pmax, pmax);
+    if (any_fail) atomicExch(st_fail, 1);
+    atomicAdd(st_flops, fl);
+  }
+}
+
+template <int PMAX>
+void run_lane(DevTree& t, const DevTree& s, const DevLists& L, int em, double eps, int be, int* p_used, int* stats,
+              cudaStream_t st) {
+  const size_t sm = lane_smem_doubles<PMAX>() * sizeof(double);
+  if (sm > 48 * 1024)
+    FMM_CUDA_TRY(cudaFuncSetAttribute(k_m2l_lane<PMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  note_launch();
+  k_m2l_lane<PMAX><<<(int)L.n_m2l_targets, 32, sm, st>>>(
+      L.m2l_tgt.ptr, L.m2l_off.ptr, L.m2l_s.ptr, t.local.ptr, s.multipole.ptr, t.tcenter.ptr, t.tbox.ptr,
+      t.tradius.ptr, t.max_influence.ptr, s.scenter.ptr, em, eps, be, p_used, stats, stats + 1,
+      reinterpret_cast<unsigned long long*>(stats + 2));
+  FMM_CUDA_TRY(cudaGetLastError());
+}
+
+}  // namespace
+
+bool launch_m2l_lane(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh, int em, double eps, int be,
+                     int* p_used, int* stats, cudaStream_t st) {
+  if (lh || p < 1 || p > kLaneMaxP) return false;
+  if (L.n_m2l_targets == 0) return true;
+  ensure_lane_tables(st);
+  switch (p) {
+    case 1: run_lane<1>(t, s, L, em, eps, be, p_used, stats, st); break;
+    case 2: run_lane<2>(t, s, L, em, eps, be, p_used, stats, st); break;
+    case 3: run_lane<3>(t, s, L, em, eps, be, p_used, stats, st); break;
+    case 4: run_lane<4>(t, s, L, em, eps, be, p_used, stats, st); break;
+    case 5: run_lane<5>(t, s, L, em, eps, be, p_used, stats, st); break;
+    case 6: run_lane<6>(t, s, L, em, eps, be, p_used, stats, st); break;
+    case 7: run_lane<7>(t, s, L, em, eps, be, p_used, stats, st); break;
+    case 8: run_lane<8>(t, s, L, em, eps, be, p_used, stats, st); break;
+    case 9: run_lane<9>(t, s, L, em, eps, be, p_used, stats, st); break;
+    case 10: run_lane<10>(t, s, L, em, eps, be, p_used, stats, st); break;
+    case 11: run_lane<11>(t, s, L, em, eps, be, p_used, stats, st); break;
+    default: run_lane<12>(t, s, L, em, eps, be, p_used, stats, st); break;
+  }
+  return true;
+}
+
+}  // namespace fmmb

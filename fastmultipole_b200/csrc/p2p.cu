@@ -5,12 +5,13 @@
 //     grad += q dx/(4 pi r^3), pairs with r^2 = 0 skipped, no hessian;
 //   vortex particle       (test/vortex.jl:83-128): u = (dx x Gamma)/(4 pi r^3)
 //     and the 9-term velocity gradient.
-// One CTA owns one target leaf (so no atomics): its targets sit in registers,
-// the bodies of each source leaf of its direct-list row are staged through
-// shared memory and broadcast to all threads.  FP64 is the drop-in arithmetic;
-// the MIXED variant moves every body relative to the target leaf centre in
-// FP64, then evaluates the kernel in FP32 (rsqrt on the SFU), summing each
-// source leaf in FP32 and the leaf partials in FP64.
+// k_p2p (direct list): one CTA per target leaf, source bodies gathered into
+// warp-private shared-memory batches, lanes split between targets and sources
+// by the leaf's size (details at the kernel).  k_direct (all pairs): one CTA
+// per block of targets, sources staged through shared memory.  FP64 is the
+// drop-in arithmetic; the MIXED variant moves every body relative to a nearby
+// centre in FP64, then evaluates the kernel in FP32 (rsqrt on the SFU),
+// summing blocks of sources in FP32 and the block partials in FP64.
 #include <algorithm>
 
 #include "context.cuh"
@@ -130,69 +131,235 @@ __device__ __forceinline__ void store(double* o, const A& acc, int k) {
     for (int a = 4; a < 13; ++a) o[a] += acc.get(k, a) * kOneOver4Pi;
 }
 
+// ---------------------------------------------------------------------------
+// Direct-list P2P.  One CTA of kWarps warps owns one direct-list row (a target leaf).
+// Each warp takes every kWarps-th source leaf of the leaf's direct-list row and
+// gathers up to Batch<KIND>::n bodies of consecutive leaves of its share (many
+// small leaves, or a piece of a large one) into its own shared-memory batch,
+// converted once per body (to FP32 relative to the target leaf centre on the
+// mixed path).  Targets sit in registers, kTPT per lane.  A target tile holds
+// up to 32 * kTPT targets; the lanes split into TS lanes along the tile times
+// 32 / TS slices along the batch, TS the smallest power of two that covers the
+// tile, so a leaf of 5 bodies keeps every lane busy as a leaf of 64 does.
+// Slices are summed by shuffles, warps through shared memory.  The mixed path
+// sums each batch in FP32 and the batches in FP64.
+constexpr int kWarps = 4;
+constexpr int kTPT = 2;
+constexpr unsigned kAll = 0xffffffffu;
+
+template <int KIND>
+struct Batch {
+  static constexpr int n = KIND == FMM_POINT_SOURCE ? 256 : 128;  // bodies per warp batch
+  static constexpr int nv = KIND == FMM_POINT_SOURCE ? 4 : 6;     // values per body: x y z + strengths
+};
+
+// accumulated channels: Laplace phi, grad (3); vortex u (3) if GS, grad u (9) if HS
+template <int KIND, bool GS, bool HS>
+__host__ __device__ constexpr int n_chan() {
+  return KIND == FMM_POINT_SOURCE ? 4 : (GS ? 3 : 0) + (HS ? 9 : 0);
+}
+// acc13 row of channel a
+template <int KIND, bool GS>
+__device__ __forceinline__ int chan_row(int a) {
+  return KIND == FMM_POINT_SOURCE ? a : (GS ? a + 1 : a + 4);
+}
+
+// one source body (x, y, z, s0, s1, s2) on one target; same arithmetic as interact()
+template <class R, int KIND, bool PS, bool GS, bool HS, int NA>
+__device__ __forceinline__ void pair1(R tx, R ty, R tz, R sx, R sy, R sz, R s0, R s1, R s2, R (&a)[NA]) {
+  R dx = tx - sx, dy = ty - sy, dz = tz - sz;
+  R r2 = dx * dx + dy * dy + dz * dz;
+  if (r2 > R(0)) {
+    R rinv = rsq(r2);
+    if (KIND == FMM_POINT_SOURCE) {
+      R qr = s0 * rinv;
+      if (PS) a[0] += qr;
+      R q3 = qr * rinv * rinv;
+      a[1] += dx * q3;
+      a[2] += dy * q3;
+      a[3] += dz * q3;
+    } else {
+      R rinv2 = rinv * rinv;
+      R den = rinv * rinv2;
+      constexpr int h = GS ? 3 : 0;
+      if (GS) {
+        a[0] += (dz * s1 - dy * s2) * den;
+        a[1] += (dx * s2 - dz * s0) * den;
+        a[2] += (dy * s0 - dx * s1) * den;
+      }
+      if (HS) {
+        R d5 = den * rinv2;
+        R cx = s1 * dz - s2 * dy, cy = s2 * dx - s0 * dz, cz = s0 * dy - s1 * dx;
+        a[(h + 0) % NA] += R(-3) * dx * cx * d5;
+        a[(h + 1) % NA] += (R(-3) * dx * cy + s2 * r2) * d5;
+        a[(h + 2) % NA] += (R(-3) * dx * cz - s1 * r2) * d5;
+        a[(h + 3) % NA] += (R(-3) * dy * cx - s2 * r2) * d5;
+        a[(h + 4) % NA] += R(-3) * dy * cy * d5;
+        a[(h + 5) % NA] += (R(-3) * dy * cz + s0 * r2) * d5;
+        a[(h + 6) % NA] += (R(-3) * dz * cx + s1 * r2) * d5;
+        a[(h + 7) % NA] += (R(-3) * dz * cy - s0 * r2) * d5;
+        a[(h + 8) % NA] += R(-3) * dz * cz * d5;
+      }
+    }
+  }
+}
+
 template <class R, int KIND, bool PS, bool GS, bool HS>
-__global__ void __launch_bounds__(kP2PThreads) k_p2p(const int* __restrict__ tgt_list, const int* __restrict__ off,
+__global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt_list, const int* __restrict__ off,
                                                      const int* __restrict__ src_of, const int* __restrict__ t_start,
                                                      const int* __restrict__ t_count, const double* __restrict__ t_center,
                                                      const int* __restrict__ s_start, const int* __restrict__ s_count,
                                                      const double4* __restrict__ tpos, const double4* __restrict__ spos,
                                                      const double4* __restrict__ sstr, double* __restrict__ acc13) {
-  constexpr int TPT = tpt<KIND>();
-  __shared__ typename Vec4<R>::T sh_p[kP2PThreads];
-  __shared__ typename Vec4<R>::T sh_s[kP2PThreads];
-  const int b = blockIdx.x;
-  const int t = tgt_list[b];
-  const int l0 = off[b], l1 = off[b + 1];
+  constexpr int NB = Batch<KIND>::n, NV = Batch<KIND>::nv, NA = n_chan<KIND, GS, HS>();
+  constexpr bool MIXED = sizeof(R) == 4;
+  extern __shared__ __align__(16) unsigned char p2p_smem[];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  R* B = reinterpret_cast<R*>(p2p_smem) + w * NV * NB;  // this warp's batch, plane v at B[v * NB]
+  double* red = reinterpret_cast<double*>(p2p_smem + kWarps * NV * NB * sizeof(R));  // [kWarps][32 kTPT][NA]
+  const int t = tgt_list[blockIdx.x];
+  const int l0 = off[blockIdx.x], l1 = off[blockIdx.x + 1];
   const int ts = t_start[t], tc = t_count[t];
-  // FP32 evaluates relative to the target leaf centre; FP64 uses absolute coordinates
-  const double ox = (sizeof(R) == 4) ? t_center[3 * t] : 0.0;
-  const double oy = (sizeof(R) == 4) ? t_center[3 * t + 1] : 0.0;
-  const double oz = (sizeof(R) == 4) ? t_center[3 * t + 2] : 0.0;
-  for (int tile = 0; tile < tc; tile += kP2PThreads * TPT) {
-    R tx[TPT], ty[TPT], tz[TPT];
-    Acc<R, TPT> acc;
-    acc.init();
-    int nt = 0;
+  const double ox = MIXED ? t_center[3 * t] : 0.0;
+  const double oy = MIXED ? t_center[3 * t + 1] : 0.0;
+  const double oz = MIXED ? t_center[3 * t + 2] : 0.0;
+  for (int tile = 0; tile < tc; tile += 32 * kTPT) {
+    const int nt = min(tc - tile, 32 * kTPT);
+    int TS = 1;
+    while (TS * kTPT < nt) TS <<= 1;
+    const int ti = lane & (TS - 1), slice = lane / TS, SS = 32 / TS;
+    R tx[kTPT], ty[kTPT], tz[kTPT];
 #pragma unroll
-    for (int k = 0; k < TPT; ++k) {
-      int i = tile + threadIdx.x + k * kP2PThreads;
+    for (int k = 0; k < kTPT; ++k) {
       tx[k] = ty[k] = tz[k] = R(0);
-      if (i < tc) {
-        double4 p = tpos[ts + i];
+      int i = ti + k * TS;
+      if (i < nt) {
+        double4 p = tpos[ts + tile + i];
         tx[k] = (R)(p.x - ox);
         ty[k] = (R)(p.y - oy);
         tz[k] = (R)(p.z - oz);
-        nt = k + 1;
       }
     }
-    for (int l = l0; l < l1; ++l) {
-      const int s = src_of[l];
-      const int ss = s_start[s], scnt = s_count[s];
-      for (int c = 0; c < scnt; c += kP2PThreads) {
-        int j = c + threadIdx.x;
-        if (j < scnt) {
-          double4 p = spos[ss + j];
-          double4 q = sstr[ss + j];
-          sh_p[threadIdx.x] = {(R)(p.x - ox), (R)(p.y - oy), (R)(p.z - oz), R(0)};
-          sh_s[threadIdx.x] = {(R)q.x, (R)q.y, (R)q.z, R(0)};
-        }
-        __syncthreads();
-        int m = min(kP2PThreads, scnt - c);
-        for (int jj = 0; jj < m; ++jj) {
-          auto P = sh_p[jj];
-          auto S = sh_s[jj];
-          interact<R, KIND, PS, GS, HS, TPT>(tx, ty, tz, nt, P.x, P.y, P.z, S.x, S.y, S.z, acc.part);
-        }
-        __syncthreads();
-      }
-      acc.flush();
-    }
+    R part[kTPT][NA];
+    double tot[kTPT][NA];
 #pragma unroll
-    for (int k = 0; k < TPT; ++k) {
-      int i = tile + threadIdx.x + k * kP2PThreads;
-      if (i < tc) store<KIND, PS, GS, HS>(acc13 + 13 * (int64_t)(ts + i), acc, k);
+    for (int k = 0; k < kTPT; ++k)
+#pragma unroll
+      for (int a = 0; a < NA; ++a) part[k][a] = R(0), tot[k][a] = 0.0;
+    int lb = l0 + w, poff = 0;  // next source leaf of this warp, bodies of it already taken
+    while (lb < l1) {
+      // candidate leaves lb + kWarps * lane; take the longest prefix that fits the batch
+      const int l = lb + kWarps * lane;
+      int cnt = 0, sb = 0;
+      if (l < l1) {
+        int s = src_of[l];
+        sb = s_start[s];
+        cnt = s_count[s];
+      }
+      if (lane == 0) {
+        sb += poff;
+        cnt -= poff;
+      }
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(kAll, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int excl = incl - cnt;
+      int nl = __popc(__ballot_sync(kAll, l < l1 && incl <= NB));
+      int nb;
+      if (nl == 0) {  // the first leaf alone overflows the batch: take NB bodies of it
+        nl = 1;
+        nb = NB;
+        poff += NB;
+      } else {
+        nb = __shfl_sync(kAll, incl, nl - 1);
+        lb += kWarps * nl;
+        poff = 0;
+      }
+      // gather: body idx of the batch lies in candidate leaf k (largest k < nl with excl_k <= idx)
+      for (int i0 = 0; i0 < nb; i0 += 32) {
+        const int idx = i0 + lane;
+        int k = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          int c = k + step;
+          int e = __shfl_sync(kAll, excl, c & 31);
+          if (c < nl && e <= idx) k = c;
+        }
+        const int ek = __shfl_sync(kAll, excl, k);
+        const int sk = __shfl_sync(kAll, sb, k);
+        if (idx < nb) {
+          const int body = sk + idx - ek;
+          double4 p = spos[body];
+          double4 q = sstr[body];
+          B[idx] = (R)(p.x - ox);
+          B[NB + idx] = (R)(p.y - oy);
+          B[2 * NB + idx] = (R)(p.z - oz);
+          B[3 * NB + idx] = (R)q.x;
+          if (NV == 6) {
+            B[(4 % NV) * NB + idx] = (R)q.y;
+            B[(5 % NV) * NB + idx] = (R)q.z;
+          }
+        }
+      }
+      __syncwarp();
+      for (int j = slice; j < nb; j += SS) {
+        const R sx = B[j], sy = B[NB + j], sz = B[2 * NB + j], s0 = B[3 * NB + j];
+        const R s1 = NV == 6 ? B[(4 % NV) * NB + j] : R(0);
+        const R s2 = NV == 6 ? B[(5 % NV) * NB + j] : R(0);
+#pragma unroll
+        for (int k = 0; k < kTPT; ++k)
+          pair1<R, KIND, PS, GS, HS, NA>(tx[k], ty[k], tz[k], sx, sy, sz, s0, s1, s2, part[k]);
+      }
+      __syncwarp();
+      if (MIXED) {
+#pragma unroll
+        for (int k = 0; k < kTPT; ++k)
+#pragma unroll
+          for (int a = 0; a < NA; ++a) tot[k][a] += (double)part[k][a], part[k][a] = R(0);
+      }
     }
+    if (!MIXED) {
+#pragma unroll
+      for (int k = 0; k < kTPT; ++k)
+#pragma unroll
+        for (int a = 0; a < NA; ++a) tot[k][a] = (double)part[k][a];
+    }
+    // slices -> lanes ti (< TS), then warps -> shared memory
+    for (int o = TS; o < 32; o <<= 1)
+#pragma unroll
+      for (int k = 0; k < kTPT; ++k)
+#pragma unroll
+        for (int a = 0; a < NA; ++a) tot[k][a] += __shfl_xor_sync(kAll, tot[k][a], o);
+    if (slice == 0) {
+#pragma unroll
+      for (int k = 0; k < kTPT; ++k) {
+        int i = ti + k * TS;
+        if (i < nt)
+#pragma unroll
+          for (int a = 0; a < NA; ++a) red[(w * 32 * kTPT + i) * NA + a] = tot[k][a];
+      }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nt * NA; e += kWarps * 32) {
+      const int i = e / NA, a = e - i * NA;
+      double v = 0;
+#pragma unroll
+      for (int q = 0; q < kWarps; ++q) v += red[(q * 32 * kTPT + i) * NA + a];
+      if (KIND == FMM_POINT_SOURCE && a == 0 && !PS) continue;
+      // atomic: under SelfTuning a non-leaf target branch and its own leaves can both own direct-list rows
+      atomicAdd(acc13 + 13 * (int64_t)(ts + tile + i) + chan_row<KIND, GS>(a), v * kOneOver4Pi);
+    }
+    __syncthreads();
   }
+}
+
+template <class R, int KIND, bool GS, bool HS>
+constexpr size_t p2p_smem_bytes() {
+  return (size_t)kWarps * Batch<KIND>::nv * Batch<KIND>::n * sizeof(R) +
+         (size_t)kWarps * 32 * kTPT * n_chan<KIND, GS, HS>() * sizeof(double);
 }
 
 // all pairs: each CTA owns kP2PThreads*TPT consecutive targets
@@ -256,8 +423,12 @@ __global__ void __launch_bounds__(kP2PThreads) k_direct(const double4* __restric
 template <class R, int KIND, bool PS, bool GS, bool HS>
 void run_p2p(const DevTree& tt, const DevTree& stt, const DevLists& L, double* acc13, cudaStream_t st) {
   if (L.n_dir_targets == 0) return;
+  constexpr size_t smem = p2p_smem_bytes<R, KIND, GS, HS>();
+  if (smem > 48 * 1024)
+    FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2p<R, KIND, PS, GS, HS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
   note_launch();
-  k_p2p<R, KIND, PS, GS, HS><<<(int)L.n_dir_targets, kP2PThreads, 0, st>>>(
+  k_p2p<R, KIND, PS, GS, HS><<<(int)L.n_dir_targets, kWarps * 32, smem, st>>>(
       L.dir_tgt.ptr, L.dir_off.ptr, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
       stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13);
   FMM_CUDA_TRY(cudaGetLastError());

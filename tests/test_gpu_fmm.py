@@ -109,6 +109,14 @@ CASES = [
                  interaction_list_method=fm.SelfTuning())),
     dict(name="clustered20k_p10", gen=lambda: clustered(20000, 2),
          kw=dict(expansion_order=10, leaf_size_source=64, multipole_acceptance=0.5)),
+    # low orders run the thread-per-pair M2L; leaves of ~5 bodies split the P2P lanes over sources
+    dict(name="uniform8k_p3_ls5", gen=lambda: uniform(8000, 4), kw=dict(expansion_order=3, leaf_size_source=5,
+                                                                       multipole_acceptance=0.6,
+                                                                       scalar_potential=True)),
+    # leaves of up to 565 bodies: several target tiles and source leaves larger than one P2P batch
+    dict(name="uniform20k_p2_ls200", gen=lambda: uniform(20000, 5), kw=dict(expansion_order=2, leaf_size_source=200,
+                                                                           multipole_acceptance=0.5,
+                                                                           scalar_potential=True)),
 ]
 
 
@@ -138,6 +146,30 @@ def test_vortex_ring_velocity_and_gradient(ctx):
     for rows in (slice(4, 7), slice(7, 16)):
         scale = np.abs(ref["out"][:, rows]).max()
         np.testing.assert_allclose(out[:, rows], ref["out"][:, rows], rtol=0, atol=1e-10 * scale)
+
+
+@pytest.mark.parametrize("p,ls", [(3, 10), (2, 200)])
+def test_vortex_low_order_and_large_leaves(ctx, p, ls):
+    buf = ring(12000, 6)
+    og, oo = opt_pair(expansion_order=p, leaf_size_source=ls, multipole_acceptance=0.5, hessian=True)
+    out, res = fm.solve_buffers(buf, L.FMM_POINT_VORTEX, og, ctx=ctx)
+    ref = O.fmm(buf, O.POINT_VORTEX, oo)
+    for rows in (slice(4, 7), slice(7, 16)):
+        scale = np.abs(ref["out"][:, rows]).max()
+        np.testing.assert_allclose(out[:, rows], ref["out"][:, rows], rtol=0, atol=1e-10 * scale)
+
+
+def test_mixed_vortex_matches_f64(ctx):
+    # FP32 near field (batch sums promoted to FP64): relative L2 deviation from the FP64 solve below 1e-5
+    buf = ring(20000, 7)
+    for ls in (80, 6):
+        og64, _ = opt_pair(expansion_order=8, leaf_size_source=ls, multipole_acceptance=0.4, hessian=True)
+        ogmx, _ = opt_pair(expansion_order=8, leaf_size_source=ls, multipole_acceptance=0.4, hessian=True,
+                           precision="mixed")
+        o64, _ = fm.solve_buffers(buf, L.FMM_POINT_VORTEX, og64, ctx=ctx)
+        omx, _ = fm.solve_buffers(buf, L.FMM_POINT_VORTEX, ogmx, ctx=ctx)
+        for rows in (slice(4, 7), slice(7, 16)):
+            assert rel_l2(omx[:, rows], o64[:, rows]) < 1e-5
 
 
 @pytest.mark.parametrize("em", [fm.PowerRelativeGradient(1e-6), fm.PowerAbsoluteGradient(1e-4),
