@@ -340,8 +340,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--bodies", type=int, default=None, help="override N (small cases for profiling)")
     args = ap.parse_args()
     w = WORKLOADS[args.config]
+    if args.bodies:
+        w = dict(w, n=args.bodies, workload=w["workload"] + f" [N overridden: {args.bodies}]")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -22,11 +22,12 @@
 //   out(m) = sum_nu [A(m) H(m, nu) w_nu / 2] (P_nu + (-1)^m Q_nu),
 // two products with constant (n+1) x (n+1) matrices per degree instead of a
 // per-pair O(n^3) matrix build and an O(n^2) application.  The constant
-// matrices B H and A H w / 2 of both magnitude sets live in constant memory;
-// every degree is a compile-time specialisation, so the expansions of a degree
-// sit in registers and the matrix entries are constant-bank operands.  The
-// rotated multipole of all degrees (needed by the coaxial step) is kept in the
-// warp's shared memory, one column per lane.
+// matrices B H and A H w / 2 of both magnitude sets live in constant memory
+// (warp-uniform reads).  The expansions of one degree sit in registers padded
+// to the kernel's maximum order, loops exit at the degree, so a single copy of
+// the code serves every degree and stays resident in the instruction cache.
+// The rotated multipole of all degrees (needed by the coaxial step) is kept in
+// the warp's shared memory, one column per lane.
 #include <mutex>
 
 #include "context.cuh"
@@ -46,21 +47,6 @@ __constant__ double c_Mt[kNhMax], c_Lt[kNhMax];
 
 __host__ __device__ constexpr int hi(int n, int m) { return n * (n + 1) / 2 + m; }
 __host__ __device__ constexpr int lenT(int n) { return n < 0 ? 0 : (n + 1) * (n + 2) * (2 * n + 3) / 6; }
-
-template <bool LOCAL>
-__device__ __forceinline__ double HB(int n, int a, int nu) {
-  if constexpr (LOCAL)
-    return c_HBe[lenT(n - 1) + a * (n + 1) + nu];
-  else
-    return c_HBz[lenT(n - 1) + a * (n + 1) + nu];
-}
-template <bool LOCAL>
-__device__ __forceinline__ double HA(int n, int m, int nu) {
-  if constexpr (LOCAL)
-    return c_HAe[lenT(n - 1) + m * (n + 1) + nu];
-  else
-    return c_HAz[lenT(n - 1) + m * (n + 1) + nu];
-}
 
 std::mutex g_tab_mu;
 bool g_tab_done[64];
@@ -103,14 +89,20 @@ void ensure_lane_tables(cudaStream_t st) {
   if (dev < 64) g_tab_done[dev] = true;
 }
 
-// rotate_y of degree N (X -> Y); LOCAL: eta set and e^{-+i nu beta}
-template <int N, bool LOCAL>
-__device__ __forceinline__ void rot_y_deg(const double (&Xr)[N + 1], const double (&Xi)[N + 1], double cb,
-                                          double sb, double (&Yr)[N + 1], double (&Yi)[N + 1]) {
-  double Rpr[N + 1], Rpi[N + 1], Rmr[N + 1], Rmi[N + 1];
-  double c = 1.0, s = 0.0;  // cos, sin (nu beta) by the reference's recurrence
+// rotate_y of degree n (X -> Y) on expansions padded to PMAX + 1 registers;
+// LOCAL: eta magnitudes and e^{-+i nu beta}.  The nu loop runs at run time
+// and fuses both matrix products (stage 2 accumulates P_nu +- Q_nu into every
+// output as soon as it is formed), so the code stays small; the unrolled a and
+// m loops are predicated at n (entries past n multiply zeros or are dropped).
+template <int PMAX, bool LOCAL>
+__device__ __forceinline__ void rot_y(int n, const double (&Xr)[PMAX + 1], const double (&Xi)[PMAX + 1], double cb,
+                                      double sb, double (&Yr)[PMAX + 1], double (&Yi)[PMAX + 1]) {
+  const int t0 = lenT(n - 1), w = n + 1;
 #pragma unroll
-  for (int nu = 0; nu <= N; ++nu) {
+  for (int m = 0; m <= PMAX; ++m) Yr[m] = Yi[m] = 0.0;
+  double c = 1.0, s = 0.0;  // cos, sin (nu beta) by the reference's recurrence
+#pragma unroll 1
+  for (int nu = 0; nu <= n; ++nu) {
     if (nu > 0) {
       const double cn = cb * c - sb * s;
       const double sn = sb * c + cb * s;
@@ -119,19 +111,21 @@ __device__ __forceinline__ void rot_y_deg(const double (&Xr)[N + 1], const doubl
     }
     double Er = 0, Ei = 0, Or = 0, Oi = 0;
 #pragma unroll
-    for (int a = 1; a <= N; ++a) {
-      const double h = HB<LOCAL>(N, a, nu);
-      if (a & 1) {
-        Or += h * Xr[a];
-        Oi += h * Xi[a];
-      } else {
-        Er += h * Xr[a];
-        Ei += h * Xi[a];
+    for (int a = 1; a <= PMAX; ++a) {
+      if (a <= n) {
+        const double h = LOCAL ? c_HBe[t0 + a * w + nu] : c_HBz[t0 + a * w + nu];
+        if (a & 1) {
+          Or += h * Xr[a];
+          Oi += h * Xi[a];
+        } else {
+          Er += h * Xr[a];
+          Ei += h * Xi[a];
+        }
       }
     }
-    const double h0 = HB<LOCAL>(N, 0, nu);
+    const double h0 = LOCAL ? c_HBe[t0 + nu] : c_HBz[t0 + nu];
     const double Zr = h0 * Xr[0], Zi = h0 * Xi[0];
-    const double sg = ((N + nu) & 1) ? -1.0 : 1.0;
+    const double sg = ((n + nu) & 1) ? -1.0 : 1.0;
     const double S1r = Er - Or, S1i = Ei - Oi;
     const double S3r = Er + Or, S3i = Ei + Oi;
     const double S2r = Zr + S3r, S2i = -(Zi + S3i);
@@ -141,22 +135,15 @@ __device__ __forceinline__ void rot_y_deg(const double (&Xr)[N + 1], const doubl
     const double ss = LOCAL ? -s : s;
     const double Pr = c * A1r - ss * A1i, Pi = c * A1i + ss * A1r;
     const double Qr = c * A3r + ss * A3i, Qi = c * A3i - ss * A3r;
-    Rpr[nu] = Pr + Qr;
-    Rpi[nu] = Pi + Qi;
-    Rmr[nu] = Pr - Qr;
-    Rmi[nu] = Pi - Qi;
-  }
+    const double Rpr = Pr + Qr, Rpi = Pi + Qi, Rmr = Pr - Qr, Rmi = Pi - Qi;
 #pragma unroll
-  for (int m = 0; m <= N; ++m) {
-    double vr = 0, vi = 0;
-#pragma unroll
-    for (int nu = 0; nu <= N; ++nu) {
-      const double h = HA<LOCAL>(N, m, nu);
-      vr += h * ((m & 1) ? Rmr[nu] : Rpr[nu]);
-      vi += h * ((m & 1) ? Rmi[nu] : Rpi[nu]);
+    for (int m = 0; m <= PMAX; ++m) {
+      if (m <= n) {
+        const double h = LOCAL ? c_HAe[t0 + m * w + nu] : c_HAz[t0 + m * w + nu];
+        Yr[m] += h * ((m & 1) ? Rmr : Rpr);
+        Yi[m] += h * ((m & 1) ? Rmi : Rpi);
+      }
     }
-    Yr[m] = vr;
-    Yi[m] = vi;
   }
 }
 
@@ -174,43 +161,50 @@ struct Pair {
 
 // rotated multipole in shared memory: plane c (re, im) of coefficient i, column lane
 __device__ __forceinline__ double& MS(double* Ms, int i, int c, int lane) { return Ms[(2 * i + c) * 32 + lane]; }
+__device__ __forceinline__ double MSr(const double* Ms, int i, int c, int lane) { return Ms[(2 * i + c) * 32 + lane]; }
 
-// rotate_z + rotate_y of degree N of the lane's multipole into shared memory;
-// returns the multipole power of degree N (rotate_z_n_power!, weight 1 for every m)
-template <int N>
-__device__ __forceinline__ double fwd_degree(const Pair& q, double* Ms, int lane, double& y0r, double& y1r,
+// rotate_z + rotate_y of degree n of the lane's multipole into shared memory;
+// returns the multipole power of degree n (rotate_z_n_power!, weight 1 for every m)
+template <int PMAX>
+__device__ __forceinline__ double fwd_degree(int n, const Pair& q, double* Ms, int lane, double& y0r, double& y1r,
                                              double& y1i) {
-  double Xr[N + 1], Xi[N + 1];
+  double Xr[PMAX + 1], Xi[PMAX + 1];
   double er = 1.0, ei = 0.0, pw = 0.0;
+  const int base = hi(n, 0);
 #pragma unroll
-  for (int a = 0; a <= N; ++a) {
-    const double2 u = __ldg(reinterpret_cast<const double2*>(q.src) + 2 * hi(N, a));
-    const double Nt = c_Mt[hi(N, a)];
+  for (int a = 0; a <= PMAX; ++a) {
+    Xr[a] = Xi[a] = 0.0;
+    if (a > n) continue;
+    const double2 u = __ldg(reinterpret_cast<const double2*>(q.src) + 2 * (base + a));
+    const double Nt = c_Mt[base + a];
     pw += (u.x * u.x + u.y * u.y) * Nt * Nt;
-    Xr[a] = N == 0 ? u.x : u.x * er - u.y * ei;
-    Xi[a] = N == 0 ? u.y : u.x * ei + u.y * er;
+    Xr[a] = n == 0 ? u.x : u.x * er - u.y * ei;
+    Xi[a] = n == 0 ? u.y : u.x * ei + u.y * er;
     const double t = er;
     er = er * q.cph - ei * q.sph;
     ei = t * q.sph + ei * q.cph;
   }
-  double Yr[N + 1], Yi[N + 1];
-  rot_y_deg<N, false>(Xr, Xi, q.cth, q.sth, Yr, Yi);
+  double Yr[PMAX + 1], Yi[PMAX + 1];
+  rot_y<PMAX, false>(n, Xr, Xi, q.cth, q.sth, Yr, Yi);
 #pragma unroll
-  for (int m = 0; m <= N; ++m) {
-    MS(Ms, hi(N, m), 0, lane) = Yr[m];
-    MS(Ms, hi(N, m), 1, lane) = Yi[m];
+  for (int m = 0; m <= PMAX; ++m) {
+    if (m > n) break;
+    MS(Ms, base + m, 0, lane) = Yr[m];
+    MS(Ms, base + m, 1, lane) = Yi[m];
   }
   y0r = Yr[0];
-  y1r = N >= 1 ? Yr[N >= 1 ? 1 : 0] : 0.0;
-  y1i = N >= 1 ? Yi[N >= 1 ? 1 : 0] : 0.0;
+  y1r = Yr[1 % (PMAX + 1)];
+  y1i = Yi[1 % (PMAX + 1)];
   return sqrt(pw);
 }
 
 // (n + m)! / t^(n + m + 1) by the reference's recurrence (src/translate.jl:184-225)
 __device__ __forceinline__ double coef0(int n, int m, double one_over_t) {
   double c = one_over_t;
+#pragma unroll 1
   for (int k = 0; k < n; ++k) c *= (k + 1) * one_over_t;
   int nm = n;
+#pragma unroll 1
   for (int j = 0; j < m; ++j) {
     nm += 1;
     c *= nm * one_over_t;
@@ -218,166 +212,142 @@ __device__ __forceinline__ double coef0(int n, int m, double one_over_t) {
   return c;
 }
 
-// local error estimate of degree N from the rotated multipole of degrees <= N
-template <int N>
-__device__ __forceinline__ double eps_local(const Pair& q, const double* Ms, int lane, bool power) {
+// local error estimate of degree n from the rotated multipole of degrees <= n
+__device__ __forceinline__ double eps_local(int n, const Pair& q, const double* Ms, int lane, bool power) {
   if (power) {
-    // degree N of translate_multipole_to_local_z_n! and local_power (src/translate.jl:238-295, :455-502)
+    // degree n of translate_multipole_to_local_z_n! and local_power (src/translate.jl:238-295, :455-502)
     double a = 0.0;
-#pragma unroll
-    for (int m = 0; m <= N; ++m) {
-      double c = coef0(N, m, q.rinv);
-      int n_np = N + m;
+#pragma unroll 1
+    for (int m = 0; m <= n; ++m) {
+      double c = coef0(n, m, q.rinv);
+      int n_np = n + m;
       double vr = 0, vi = 0;
-#pragma unroll
-      for (int np = m; np <= N; ++np) {
-        vr += c * Ms[(2 * hi(np, m)) * 32 + lane];
-        vi += c * Ms[(2 * hi(np, m) + 1) * 32 + lane];
+#pragma unroll 1
+      for (int np = m; np <= n; ++np) {
+        vr += c * MSr(Ms, hi(np, m), 0, lane);
+        vi += c * MSr(Ms, hi(np, m), 1, lane);
         n_np += 1;
         c *= n_np * q.rinv;
       }
-      const double Nt = c_Lt[hi(N, m)];
+      const double Nt = c_Lt[hi(n, m)];
       a += (vr * vr + vi * vi) * Nt * Nt;
     }
     const double lphi = sqrt(a);
-    return 1.7320508075688772 * lphi * q.r_l_nm1 * q.nm1_fact_inv / c_Lt[hi(N, 0)];
+    return 1.7320508075688772 * lphi * q.r_l_nm1 * q.nm1_fact_inv / c_Lt[hi(n, 0)];
   }
   // translate_multipole_to_local_z_m01_n (src/translate.jl:302-364)
   double c = q.n_fact_t_np1;
-  int n_np = N;
+  int n_np = n;
   double a0 = 0;
-#pragma unroll
-  for (int np = 0; np <= N; ++np) {
-    a0 += c * Ms[(2 * hi(np, 0)) * 32 + lane];
+#pragma unroll 1
+  for (int np = 0; np <= n; ++np) {
+    a0 += c * MSr(Ms, hi(np, 0), 0, lane);
     n_np += 1;
     c *= n_np * q.rinv;
   }
-  c = q.n_fact_t_np1 * ((N + 1) * q.rinv);
-  n_np = N + 1;
+  c = q.n_fact_t_np1 * ((n + 1) * q.rinv);
+  n_np = n + 1;
   double b1r = 0, b1i = 0;
-#pragma unroll
-  for (int np = 1; np <= N; ++np) {
-    b1r += c * Ms[(2 * hi(np, 1)) * 32 + lane];
-    b1i += c * Ms[(2 * hi(np, 1) + 1) * 32 + lane];
+#pragma unroll 1
+  for (int np = 1; np <= n; ++np) {
+    b1r += c * MSr(Ms, hi(np, 1), 0, lane);
+    b1i += c * MSr(Ms, hi(np, 1), 1, lane);
     n_np += 1;
     c *= n_np * q.rinv;
   }
   return (fabs(b1r) + fabs(b1i) + fabs(a0)) * q.r_l_nm1 * q.nm1_fact_inv;
 }
 
-// error-controlled degrees N..PMAX: the reference's degree loop, one degree per
-// specialisation, until every lane has met its tolerance or PMAX is reached
-template <int N, int PMAX>
-__device__ __forceinline__ void err_loop(Pair& q, double* Ms, int lane, bool power, int be) {
-  if constexpr (N <= PMAX) {
-    if (!__any_sync(kAll, q.active)) return;
-    if (q.active) {
-      double y0r, y1r, y1i;
-      const double pn_phi = fwd_degree<N>(q, Ms, lane, y0r, y1r, y1i);
-      const double Mn0_next = c_Mt[hi(N, 0)];
-      double eps_mp;
-      if (power)
-        eps_mp = 1.7320508075688772 * q.mp_phi * q.r_mp_inv_np2 * q.np1_fact / q.Mn0;
-      else
-        eps_mp = (sqrt(y1r * y1r + y1i * y1i) + fabs(y0r)) * q.np1_fact * q.r_mp_inv_np2;
-      if (eps_mp <= q.thr) {
-        const double eps_l = eps_local<N>(q, Ms, lane, power);
-        if (eps_mp + eps_l * 2.0 <= q.thr) {
-          q.P = N - 1 + (be ? 1 : 0);
-          q.ok = true;
-          q.active = false;
-        }
-      }
-      if (q.active) {
-        if (power || N < PMAX) {
-          q.n_fact_t_np1 *= (N + 1) * q.rinv;
-          q.r_l_nm1 *= q.r_l;
-          q.r_mp_inv_np2 *= q.r_mp_inv;
-          q.nm1_fact_inv /= N;
-          q.np1_fact *= N + 1;
-        }
-        if (power) {
-          q.mp_phi = pn_phi;
-          q.Mn0 = Mn0_next;
-        }
-      }
+// one degree of the reference's error-controlled loop (src/translate.jl:1124-1412,
+// :555-829) after degree n of the rotated multipole is in shared memory
+template <int PMAX>
+__device__ __forceinline__ void err_step(int n, Pair& q, const double* Ms, int lane, bool power, int be,
+                                         double pn_phi, double y0r, double y1r, double y1i) {
+  const double Mn0_next = c_Mt[hi(n, 0)];
+  double eps_mp;
+  if (power)
+    eps_mp = 1.7320508075688772 * q.mp_phi * q.r_mp_inv_np2 * q.np1_fact / q.Mn0;
+  else
+    eps_mp = (sqrt(y1r * y1r + y1i * y1i) + fabs(y0r)) * q.np1_fact * q.r_mp_inv_np2;
+  if (eps_mp <= q.thr) {
+    const double eps_l = eps_local(n, q, Ms, lane, power);
+    if (eps_mp + eps_l * 2.0 <= q.thr) {
+      q.P = n - 1 + (be ? 1 : 0);
+      q.ok = true;
+      q.active = false;
+      return;
     }
-    err_loop<N + 1, PMAX>(q, Ms, lane, power, be);
+  }
+  if (power || n < PMAX) {
+    q.n_fact_t_np1 *= (n + 1) * q.rinv;
+    q.r_l_nm1 *= q.r_l;
+    q.r_mp_inv_np2 *= q.r_mp_inv;
+    q.nm1_fact_inv /= n;
+    q.np1_fact *= n + 1;
+  }
+  if (power) {
+    q.mp_phi = pn_phi;
+    q.Mn0 = Mn0_next;
   }
 }
 
-// all degrees N..PMAX without error control
-template <int N, int PMAX>
-__device__ __forceinline__ void plain_loop(const Pair& q, double* Ms, int lane) {
-  if constexpr (N <= PMAX) {
-    if (q.valid) {
-      double y0r, y1r, y1i;
-      fwd_degree<N>(q, Ms, lane, y0r, y1r, y1i);
-    }
-    plain_loop<N + 1, PMAX>(q, Ms, lane);
-  }
-}
-
-// degree N of the local expansion: coaxial translation of the rotated multipole
+// degree n of the local expansion: coaxial translation of the rotated multipole
 // (sources m..P), rotate_y back, back_rotate_z, then the sum over the 32 lanes
 // into the warp accumulator (stage: 2 (PMAX+1) rows of 33 doubles)
-template <int N, int PMAX>
-__device__ __forceinline__ void back_loop(const Pair& q, const double* Ms, double* stage, double* acc, int lane,
-                                          int pwarp) {
-  if constexpr (N <= PMAX) {
-    if (N > pwarp) return;
-    const bool on = q.valid && N <= q.P;
-    double Xr[N + 1], Xi[N + 1];
+template <int PMAX>
+__device__ __forceinline__ void back_degree(int n, const Pair& q, const double* Ms, double* stage, double* acc,
+                                            int lane) {
+  const bool on = q.valid && n <= q.P;
+  double Xr[PMAX + 1], Xi[PMAX + 1];
 #pragma unroll
-    for (int m = 0; m <= N; ++m) {
-      double c = coef0(N, m, q.rinv);
-      int n_np = N + m;
-      double vr = 0, vi = 0;
-#pragma unroll
-      for (int np = m; np <= PMAX; ++np) {
-        if (np <= q.P) {
-          vr += c * Ms[(2 * hi(np, m)) * 32 + lane];
-          vi += c * Ms[(2 * hi(np, m) + 1) * 32 + lane];
-        }
-        n_np += 1;
-        c *= n_np * q.rinv;
-      }
-      Xr[m] = on ? vr : 0.0;
-      Xi[m] = on ? vi : 0.0;
+  for (int m = 0; m <= PMAX; ++m) {
+    Xr[m] = Xi[m] = 0.0;
+    if (m > n) continue;
+    double c = coef0(n, m, q.rinv);
+    int n_np = n + m;
+    double vr = 0, vi = 0;
+    const int top = on ? q.P : m - 1;
+#pragma unroll 1
+    for (int np = m; np <= top; ++np) {
+      vr += c * MSr(Ms, hi(np, m), 0, lane);
+      vi += c * MSr(Ms, hi(np, m), 1, lane);
+      n_np += 1;
+      c *= n_np * q.rinv;
     }
-    double Yr[N + 1], Yi[N + 1];
-    rot_y_deg<N, true>(Xr, Xi, q.cth, q.sth, Yr, Yi);
-    double er = 1.0, ei = 0.0;
-#pragma unroll
-    for (int m = 0; m <= N; ++m) {
-      const double cr = er, ci = -ei;
-      const double vr = N == 0 ? Yr[m] : Yr[m] * cr - Yi[m] * ci;
-      const double vi = N == 0 ? Yi[m] : Yr[m] * ci + Yi[m] * cr;
-      stage[(2 * m) * 33 + lane] = on ? vr : 0.0;
-      stage[(2 * m + 1) * 33 + lane] = on ? vi : 0.0;
-      const double t = er;
-      er = er * q.cph - ei * q.sph;
-      ei = t * q.sph + ei * q.cph;
-    }
-    __syncwarp();
-    if (lane < 2 * (N + 1)) {
-      double v = 0.0;
-#pragma unroll 8
-      for (int k = 0; k < 32; ++k) v += stage[lane * 33 + k];
-      acc[2 * hi(N, 0) + lane] += v;
-    }
-    __syncwarp();
-    back_loop<N + 1, PMAX>(q, Ms, stage, acc, lane, pwarp);
+    Xr[m] = vr;
+    Xi[m] = vi;
   }
+  double Yr[PMAX + 1], Yi[PMAX + 1];
+  rot_y<PMAX, true>(n, Xr, Xi, q.cth, q.sth, Yr, Yi);
+  double er = 1.0, ei = 0.0;
+#pragma unroll
+  for (int m = 0; m <= PMAX; ++m) {
+    if (m > n) break;
+    const double cr = er, ci = -ei;
+    const double vr = n == 0 ? Yr[m] : Yr[m] * cr - Yi[m] * ci;
+    const double vi = n == 0 ? Yi[m] : Yr[m] * ci + Yi[m] * cr;
+    stage[(2 * m) * 33 + lane] = on ? vr : 0.0;
+    stage[(2 * m + 1) * 33 + lane] = on ? vi : 0.0;
+    const double t = er;
+    er = er * q.cph - ei * q.sph;
+    ei = t * q.sph + ei * q.cph;
+  }
+  __syncwarp();
+  if (lane < 2 * (n + 1)) {
+    double v = 0.0;
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) v += stage[lane * 33 + k];
+    acc[2 * hi(n, 0) + lane] += v;
+  }
+  __syncwarp();
 }
 
 __device__ __forceinline__ unsigned long long lane_pair_flops(int P) {
   // the reference's operation count: 4 [2 sum_n (n+1)(2n+1) + sum_n sum_m (P-m+1)]
-  unsigned long long rot = 0, coax = 0;
-  for (int n = 0; n <= P; ++n) {
-    rot += (unsigned long long)(n + 1) * (2 * n + 1);
-    for (int m = 0; m <= n; ++m) coax += (unsigned long long)(P - m + 1);
-  }
+  // closed forms: sum_n (n+1)(2n+1) = P(P+1)(2P+1)/3 + 3P(P+1)/2 + P+1, sum_m (P-m+1)^2 = (P+1)(P+2)(2P+3)/6
+  const unsigned long long p = (unsigned long long)P;
+  const unsigned long long rot = p * (p + 1) * (2 * p + 1) / 3 + 3 * p * (p + 1) / 2 + p + 1;
+  const unsigned long long coax = (p + 1) * (p + 2) * (2 * p + 3) / 6;
   return 4ull * (2 * rot + coax);
 }
 
@@ -476,21 +446,24 @@ __global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_lis
         q.active = true;
       }
     }
-    if (errc) {
-      if (q.valid) {
-        double y0r, y1r, y1i;
-        fwd_degree<0>(q, Ms, lane, y0r, y1r, y1i);
-      }
-      err_loop<1, PMAX>(q, Ms, lane, power, be);
-      if (q.active) q.active = false;  // PMAX reached: P = PMAX, tolerance missed
-    } else {
-      plain_loop<0, PMAX>(q, Ms, lane);
+    // degree 0 for every valid lane, then degree by degree while a lane is active
+    // (error control) or up to PMAX (plain)
+    q.active = q.valid;
+#pragma unroll 1
+    for (int n = 0; n <= PMAX; ++n) {
+      if (!__any_sync(kAll, q.active)) break;
+      if (!q.active) continue;
+      double y0r, y1r, y1i;
+      const double pn_phi = fwd_degree<PMAX>(n, q, Ms, lane, y0r, y1r, y1i);
+      if (errc && n > 0) err_step<PMAX>(n, q, Ms, lane, power, be, pn_phi, y0r, y1r, y1i);
     }
+    q.active = false;  // error control: lanes still active reached PMAX (P = PMAX, tolerance missed)
     int pw = q.valid ? q.P : -1;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) pw = max(pw, __shfl_xor_sync(kAll, pw, o));
     __syncwarp();
-    back_loop<0, PMAX>(q, Ms, stage, acc, lane, pw);
+#pragma unroll 1
+    for (int n = 0; n <= pw; ++n) back_degree<PMAX>(n, q, Ms, stage, acc, lane);
     if (q.valid) {
       if (p_used) p_used[l] = q.P;
       pmax = max(pmax, q.P);

@@ -134,7 +134,7 @@ __device__ __forceinline__ void store(double* o, const A& acc, int k) {
 // ---------------------------------------------------------------------------
 // Direct-list P2P.  One CTA of kWarps warps owns one direct-list row (a target leaf).
 // Each warp takes every kWarps-th source leaf of the leaf's direct-list row and
-// gathers up to Batch<KIND>::n bodies of consecutive leaves of its share (many
+// gathers up to batch_bodies() bodies of consecutive leaves of its share (many
 // small leaves, or a piece of a large one) into its own shared-memory batch,
 // converted once per body (to FP32 relative to the target leaf centre on the
 // mixed path).  Targets sit in registers, kTPT per lane.  A target tile holds
@@ -152,6 +152,23 @@ struct Batch {
   static constexpr int n = KIND == FMM_POINT_SOURCE ? 256 : 128;  // bodies per warp batch
   static constexpr int nv = KIND == FMM_POINT_SOURCE ? 4 : 6;     // values per body: x y z + strengths
 };
+
+// FP32 point sources evaluate two targets per lane with packed f32x2 arithmetic;
+// their batch holds per body {-x, -x, -y, -y}, {-z, -z, q, q} (ready-made pairs)
+template <class R, int KIND>
+__host__ __device__ constexpr bool packed() { return sizeof(R) == 4 && KIND == FMM_POINT_SOURCE; }
+template <class R, int KIND>
+__host__ __device__ constexpr int slots_per_body() { return packed<R, KIND>() ? 8 : Batch<KIND>::nv; }
+// bodies per warp batch: the packed batch is halved to keep the same shared memory per CTA
+template <class R, int KIND>
+__host__ __device__ constexpr int batch_bodies() { return packed<R, KIND>() ? 128 : Batch<KIND>::n; }
+
+// 1/sqrt(x) on the SFU, denormal inputs flushed (rsqrt.approx.ftz.f32)
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 
 // accumulated channels: Laplace phi, grad (3); vortex u (3) if GS, grad u (9) if HS
 template <int KIND, bool GS, bool HS>
@@ -211,12 +228,15 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
                                                      const int* __restrict__ s_start, const int* __restrict__ s_count,
                                                      const double4* __restrict__ tpos, const double4* __restrict__ spos,
                                                      const double4* __restrict__ sstr, double* __restrict__ acc13) {
-  constexpr int NB = Batch<KIND>::n, NV = Batch<KIND>::nv, NA = n_chan<KIND, GS, HS>();
+  constexpr int NB = batch_bodies<R, KIND>(), NV = Batch<KIND>::nv, NA = n_chan<KIND, GS, HS>();
+  constexpr int NS = slots_per_body<R, KIND>();
   constexpr bool MIXED = sizeof(R) == 4;
+  constexpr bool PACK = packed<R, KIND>();
+  static_assert(!PACK || kTPT == 2, "packed path pairs two targets per lane");
   extern __shared__ __align__(16) unsigned char p2p_smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  R* B = reinterpret_cast<R*>(p2p_smem) + w * NV * NB;  // this warp's batch, plane v at B[v * NB]
-  double* red = reinterpret_cast<double*>(p2p_smem + kWarps * NV * NB * sizeof(R));  // [kWarps][32 kTPT][NA]
+  R* B = reinterpret_cast<R*>(p2p_smem) + w * NS * NB;  // this warp's batch, plane v at B[v * NB]
+  double* red = reinterpret_cast<double*>(p2p_smem + kWarps * NS * NB * sizeof(R));  // [kWarps][32 kTPT][NA]
   const int t = tgt_list[blockIdx.x];
   const int l0 = off[blockIdx.x], l1 = off[blockIdx.x + 1];
   const int ts = t_start[t], tc = t_count[t];
@@ -290,7 +310,14 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
         }
         const int ek = __shfl_sync(kAll, excl, k);
         const int sk = __shfl_sync(kAll, sb, k);
-        if (idx < nb) {
+        if (PACK && idx < nb) {
+          const int body = sk + idx - ek;
+          const double4 p = spos[body];
+          const float x = -(float)(p.x - ox), y = -(float)(p.y - oy), z = -(float)(p.z - oz), q = (float)sstr[body].x;
+          float4* B4 = reinterpret_cast<float4*>(B);
+          B4[2 * idx] = make_float4(x, x, y, y);
+          B4[2 * idx + 1] = make_float4(z, z, q, q);
+        } else if (idx < nb) {
           const int body = sk + idx - ek;
           double4 p = spos[body];
           double4 q = sstr[body];
@@ -305,13 +332,49 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
         }
       }
       __syncwarp();
-      for (int j = slice; j < nb; j += SS) {
-        const R sx = B[j], sy = B[NB + j], sz = B[2 * NB + j], s0 = B[3 * NB + j];
-        const R s1 = NV == 6 ? B[(4 % NV) * NB + j] : R(0);
-        const R s2 = NV == 6 ? B[(5 % NV) * NB + j] : R(0);
+      if constexpr (PACK) {
+        // targets 0 and 1 of the lane in the two halves of every f32x2 operation
+        const float4* B4 = reinterpret_cast<const float4*>(B);
+        const float2 tx2 = make_float2((float)tx[0], (float)tx[1]);
+        const float2 ty2 = make_float2((float)ty[0], (float)ty[1]);
+        const float2 tz2 = make_float2((float)tz[0], (float)tz[1]);
+        float2 ph = make_float2(0.f, 0.f), gx = ph, gy = ph, gz = ph;
+#pragma unroll 4
+        for (int j = slice; j < nb; j += SS) {
+          const float4 u = B4[2 * j], v = B4[2 * j + 1];
+          const float2 dx = __fadd2_rn(tx2, make_float2(u.x, u.y));
+          const float2 dy = __fadd2_rn(ty2, make_float2(u.z, u.w));
+          const float2 dz = __fadd2_rn(tz2, make_float2(v.x, v.y));
+          float2 r2 = __fmul2_rn(dx, dx);
+          r2 = __ffma2_rn(dy, dy, r2);
+          r2 = __ffma2_rn(dz, dz, r2);
+          float2 ri;
+          ri.x = r2.x > 0.f ? rsqrt_ftz(r2.x) : 0.f;  // coincident bodies are skipped
+          ri.y = r2.y > 0.f ? rsqrt_ftz(r2.y) : 0.f;
+          const float2 qr = __fmul2_rn(make_float2(v.z, v.w), ri);
+          ph = __fadd2_rn(ph, qr);
+          const float2 q3 = __fmul2_rn(__fmul2_rn(qr, ri), ri);
+          gx = __ffma2_rn(dx, q3, gx);
+          gy = __ffma2_rn(dy, q3, gy);
+          gz = __ffma2_rn(dz, q3, gz);
+        }
+        part[0][0] += (R)ph.x;
+        part[1][0] += (R)ph.y;
+        part[0][1 % NA] += (R)gx.x;
+        part[1][1 % NA] += (R)gx.y;
+        part[0][2 % NA] += (R)gy.x;
+        part[1][2 % NA] += (R)gy.y;
+        part[0][3 % NA] += (R)gz.x;
+        part[1][3 % NA] += (R)gz.y;
+      } else {
+        for (int j = slice; j < nb; j += SS) {
+          const R sx = B[j], sy = B[NB + j], sz = B[2 * NB + j], s0 = B[3 * NB + j];
+          const R s1 = NV == 6 ? B[(4 % NV) * NB + j] : R(0);
+          const R s2 = NV == 6 ? B[(5 % NV) * NB + j] : R(0);
 #pragma unroll
-        for (int k = 0; k < kTPT; ++k)
-          pair1<R, KIND, PS, GS, HS, NA>(tx[k], ty[k], tz[k], sx, sy, sz, s0, s1, s2, part[k]);
+          for (int k = 0; k < kTPT; ++k)
+            pair1<R, KIND, PS, GS, HS, NA>(tx[k], ty[k], tz[k], sx, sy, sz, s0, s1, s2, part[k]);
+        }
       }
       __syncwarp();
       if (MIXED) {
@@ -358,7 +421,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
 
 template <class R, int KIND, bool GS, bool HS>
 constexpr size_t p2p_smem_bytes() {
-  return (size_t)kWarps * Batch<KIND>::nv * Batch<KIND>::n * sizeof(R) +
+  return (size_t)kWarps * slots_per_body<R, KIND>() * batch_bodies<R, KIND>() * sizeof(R) +
          (size_t)kWarps * 32 * kTPT * n_chan<KIND, GS, HS>() * sizeof(double);
 }
 

@@ -79,14 +79,22 @@ __global__ void k_bbox_partial(const double4* __restrict__ pos, int64_t n, doubl
 }
 
 // center_box / get_center_box (src/tree.jl:894-924) and the cubic root cell (src/tree.jl:20-26)
+// one warp: lanes reduce strided partials, then shuffles (min/max are exact in any order)
 __global__ void k_bbox_final(const double* __restrict__ part, int nb, RootGeom* root) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (blockIdx.x != 0) return;
+  const int lane = threadIdx.x;
   double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for (int b = 0; b < nb; ++b)
+  for (int b = lane; b < nb; b += 32)
     for (int k = 0; k < 3; ++k) {
       mn[k] = fmin(mn[k], part[6 * b + k]);
       mx[k] = fmax(mx[k], part[6 * b + 3 + k]);
     }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 3; ++k) {
+      mn[k] = fmin(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+      mx[k] = fmax(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+    }
+  if (lane != 0) return;
   double box[3];
   for (int k = 0; k < 3; ++k) {
     root->c[k] = (mx[k] + mn[k]) * 0.5;
@@ -444,7 +452,7 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
   FMM_CHECK(leaf_size >= 1, FMM_ERR_ARGUMENT, "leaf_size must be >= 1");
 
   // root cell
-  int nb_part = blocks_for(n);
+  int nb_part = (int)std::min<int64_t>(blocks_for(n), 148 * 8);
   sc.tmp_d.grow(6 * (size_t)nb_part + 8);
   double* part = sc.tmp_d.ptr;
   RootGeom* root = reinterpret_cast<RootGeom*>(part + 6 * nb_part);
