@@ -141,7 +141,7 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
     e.scalar_potential = 1;
     e.gradient = 1;
     e.hessian = 0;
-    e.precision = FMM_PRECISION_F64;
+    e.precision = o.precision;  // the mixed solve estimates with its FP32 near field
     int64_t nt = in.tpos ? in.n_t : in.n_s;
     c->est_out16.grow(16 * (size_t)nt);
     run_fmm(c, c->est, in, e, c->est_out16.ptr, nullptr, true);

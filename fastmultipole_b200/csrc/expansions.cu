@@ -292,8 +292,9 @@ void dispatch_slots(int p, bool lh, F& f) {
 
 // ---------------------------------------------------------------------------
 // P2M: body_to_multipole! of Point{Source} / Point{Vortex}
-// (src/bodytomultipole.jl:112-139, 283-334, 387-489); warp per leaf, lanes over m
-// for the harmonics recursion, lanes over (n, m) for the accumulation.
+// (src/bodytomultipole.jl:112-139, 283-334, 387-489).  The unit operator below
+// uses one warp per expansion, lanes over m for the harmonics recursion and over
+// (n, m) for the accumulation; the tree pass uses k_p2m_lane (lane per body).
 __device__ __forceinline__ void q_nm1(const double* h, int n, int m, double _1_m, double* o) {
   int i = (n - 1) * n / 2 + m;  // index of (n-1, m)
   if (m > 0) {
@@ -408,27 +409,172 @@ __device__ __forceinline__ void p2m_body(double (&acc)[kSlots][4], double* h, in
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(32 * kWarps) k_p2m(const int* __restrict__ leaf_index, int n_leaves,
-                                                     const int* __restrict__ body_start,
-                                                     const int* __restrict__ body_count,
-                                                     const double* __restrict__ scen, const double4* __restrict__ pos,
-                                                     const double4* __restrict__ str, double* __restrict__ M, int p,
-                                                     int kind) {
+// P2M, one warp per leaf and one lane per body (32 bodies at a time): each lane
+// runs the regular-harmonic recurrence of calculate_q! (src/bodytomultipole.jl:
+// 112-139) for its body, degree n from degree n-1 in registers, forms the
+// degree-n contributions of body_to_multipole! (source: :283-334, vortex:
+// :387-489), and the 32 lanes' contributions are summed column by column through
+// shared memory into the leaf's multipole (the warp owns the leaf: no atomics).
+template <int PMAX, bool VORTEX>
+__global__ void __launch_bounds__(32 * kWarps) k_p2m_lane(const int* __restrict__ leaf_index, int n_leaves,
+                                                          const int* __restrict__ body_start,
+                                                          const int* __restrict__ body_count,
+                                                          const double* __restrict__ scen,
+                                                          const double4* __restrict__ pos,
+                                                          const double4* __restrict__ str, double* __restrict__ M) {
+  constexpr int NC = VORTEX ? 4 : 2;  // doubles per coefficient written
+  constexpr int ROWS = NC * (PMAX + 1);
   extern __shared__ double smem[];
-  const int wid = threadIdx.x >> 5;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int w = blockIdx.x * kWarps + wid;
   if (w >= n_leaves) return;
-  double* h = smem + wid * 2 * nh(p);
+  double* stage = smem + wid * ROWS * 33;
   const int b = leaf_index[w];
   const int s0 = body_start[b], cnt = body_count[b];
-  double c[3] = {scen[3 * b], scen[3 * b + 1], scen[3 * b + 2]};
-  double acc[kSlots][4];
-  acc_zero(acc);
-  for (int j = 0; j < cnt; ++j) {
-    double4 x = pos[s0 + j];
-    p2m_body(acc, h, kind, x.x - c[0], x.y - c[1], x.z - c[2], str[s0 + j], p);
+  const double cx = scen[3 * b], cy = scen[3 * b + 1], cz = scen[3 * b + 2];
+  double* Mb = M + (int64_t)4 * ((PMAX + 1) * (PMAX + 2) / 2) * b;
+  for (int j0 = 0; j0 < cnt; j0 += 32) {
+    const int j = j0 + lane;
+    const bool valid = j < cnt;
+    double dx = 0, dy = 0, dz = 0;
+    double4 sv = make_double4(0, 0, 0, 0);
+    if (valid) {
+      const double4 x = pos[s0 + j];
+      dx = x.x - cx;
+      dy = x.y - cy;
+      dz = x.z - cz;
+      sv = str[s0 + j];
+    }
+    // calculate_q! arguments: source (dx/2, dy/2, dx/2, -dy/2, dz), vortex (-dx/2, -dy/2, -dx/2, dy/2, -dz)
+    const double xr = VORTEX ? -dx * 0.5 : dx * 0.5, xi = VORTEX ? -dy * 0.5 : dy * 0.5;
+    const double er = xr, ei = -xi, z = VORTEX ? -dz : dz;
+    double Hr[PMAX + 1], Hi[PMAX + 1], Pr[PMAX + 1], Pi[PMAX + 1];
+#pragma unroll
+    for (int m = 0; m <= PMAX; ++m) Hr[m] = Hi[m] = Pr[m] = Pi[m] = 0.0;
+    Hr[0] = 1.0;
+#pragma unroll 1
+    for (int n = 0; n <= PMAX; ++n) {
+      if (n > 0) {
+#pragma unroll
+        for (int m = 0; m <= PMAX; ++m) {
+          Pr[m] = Hr[m];
+          Pi[m] = Hi[m];
+        }
+        // q_nm1: (n-1, m-1) [m = 0: -conj-mirror of (n-1, 1)], (n-1, m), (n-1, m+1)
+#pragma unroll
+        for (int m = 0; m <= PMAX; ++m) {
+          if (m > n) continue;
+          double q0, q1;
+          if (m > 0) {
+            q0 = Pr[m > 0 ? m - 1 : 0];
+            q1 = Pi[m > 0 ? m - 1 : 0];
+          } else {
+            q0 = n > 1 ? -Pr[1 % (PMAX + 1)] : 0.0;
+            q1 = n > 1 ? Pi[1 % (PMAX + 1)] : 0.0;
+          }
+          const double q2 = m < n ? Pr[m] : 0.0, q3 = m < n ? Pi[m] : 0.0;
+          const double q4 = (m + 1 <= PMAX && m + 1 < n) ? Pr[(m + 1) % (PMAX + 1)] : 0.0;
+          const double q5 = (m + 1 <= PMAX && m + 1 < n) ? Pi[(m + 1) % (PMAX + 1)] : 0.0;
+          Hr[m] = (-(xr * q1 + xi * q0) - (er * q5 + ei * q4) - z * q2) / n;
+          Hi[m] = ((xr * q0 - xi * q1) + (er * q4 - ei * q5) - z * q3) / n;
+        }
+      }
+      // degree-n contributions of this lane's body
+#pragma unroll
+      for (int m = 0; m <= PMAX; ++m) {
+        if (m > n) continue;
+        double v0, v1, v2 = 0, v3 = 0;
+        const double _1_m = (m & 1) ? -1.0 : 1.0;
+        if (!VORTEX) {
+          const double sg = ((n + m) & 1) ? -1.0 : 1.0, strength = -sv.x;
+          v0 = Hr[m] * sg * strength;
+          v1 = -(Hi[m] * sg * strength);
+        } else {
+          // q_n: (n, m-1) [m = 0: mirror of (n, 1)], (n, m), (n, m+1)
+          double q0, q1;
+          if (m > 0) {
+            q0 = Hr[m > 0 ? m - 1 : 0];
+            q1 = Hi[m > 0 ? m - 1 : 0];
+          } else {
+            q0 = n > 0 ? -_1_m * Hr[1 % (PMAX + 1)] : 0.0;
+            q1 = n > 0 ? _1_m * Hi[1 % (PMAX + 1)] : 0.0;
+          }
+          const double q2 = Hr[m], q3 = Hi[m];
+          const double q4 = (m + 1 <= PMAX && m < n) ? Hr[(m + 1) % (PMAX + 1)] : 0.0;
+          const double q5 = (m + 1 <= PMAX && m < n) ? Hi[(m + 1) % (PMAX + 1)] : 0.0;
+          const double vx = sv.x, vy = sv.y, vz = sv.z;
+          const double a = (double)(n - m + 1) * 0.5, bb = (double)(n + m + 1) * 0.5, _1_np1 = 1.0 / (n + 1);
+          v0 = _1_m * ((-vx * q0 + vy * q1) * a + (vx * q4 + vy * q5) * bb - vz * m * q3) * _1_np1;
+          v1 = _1_m * ((vx * q1 + vy * q0) * a + (-vx * q5 + vy * q4) * bb - vz * m * q2) * _1_np1;
+          if (n >= 1) {
+            double r0, r1;
+            if (m > 0) {
+              r0 = Pr[m > 0 ? m - 1 : 0];
+              r1 = Pi[m > 0 ? m - 1 : 0];
+            } else {
+              r0 = n > 1 ? -_1_m * Pr[1 % (PMAX + 1)] : 0.0;
+              r1 = n > 1 ? _1_m * Pi[1 % (PMAX + 1)] : 0.0;
+            }
+            const double r2 = m < n ? Pr[m] : 0.0, r3 = m < n ? Pi[m] : 0.0;
+            const double r4 = (m + 1 <= PMAX && m + 1 < n) ? Pr[(m + 1) % (PMAX + 1)] : 0.0;
+            const double r5 = (m + 1 <= PMAX && m + 1 < n) ? Pi[(m + 1) % (PMAX + 1)] : 0.0;
+            const double _1_over_n = 1.0 / n;
+            v2 = -(_1_m * _1_over_n * (0.5 * (-vy * r0 - vx * r1 + vy * r4 - vx * r5) - vz * r2));
+            v3 = -(_1_m * _1_over_n * (0.5 * (vy * r1 - vx * r0 - vy * r5 - vx * r4) + vz * r3));
+          }
+        }
+        stage[(NC * m) * 33 + lane] = valid ? v0 : 0.0;
+        stage[(NC * m + 1) * 33 + lane] = valid ? v1 : 0.0;
+        if (VORTEX) {
+          stage[((NC * m + 2) % ROWS) * 33 + lane] = valid ? v2 : 0.0;
+          stage[((NC * m + 3) % ROWS) * 33 + lane] = valid ? v3 : 0.0;
+        }
+      }
+      __syncwarp();
+      const int hn = n * (n + 1) / 2;
+      for (int v = lane; v < NC * (n + 1); v += 32) {
+        double t = 0.0;
+#pragma unroll 8
+        for (int k = 0; k < 32; ++k) t += stage[v * 33 + k];
+        Mb[4 * (hn + v / NC) + v % NC] += t;
+      }
+      __syncwarp();
+    }
   }
-  acc_store_add(M + 4 * nh(p) * b, acc, p, kind == FMM_POINT_VORTEX);
+}
+
+template <bool VORTEX>
+struct P2MLaneLaunch {
+  DevTree& s;
+  cudaStream_t st;
+  template <int PMAX>
+  void go() {
+    constexpr size_t sm = (size_t)kWarps * (VORTEX ? 4 : 2) * (PMAX + 1) * 33 * sizeof(double);
+    if (sm > 48 * 1024)
+      FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_lane<PMAX, VORTEX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sm));
+    int g = (int)((s.n_leaves + kWarps - 1) / kWarps);
+    note_launch();
+    k_p2m_lane<PMAX, VORTEX><<<g, 32 * kWarps, sm, st>>>(s.leaf_index.ptr, (int)s.n_leaves, s.body_start.ptr,
+                                                           s.body_count.ptr, s.scenter.ptr, s.pos.ptr, s.str.ptr,
+                                                           s.multipole.ptr);
+    FMM_CUDA_TRY(cudaGetLastError());
+  }
+};
+
+template <class F>
+void dispatch_order(int p, F& f) {
+  switch (p) {
+#define FMM_P(PP) \
+  case PP:        \
+    f.template go<PP>(); \
+    break;
+    FMM_P(0) FMM_P(1) FMM_P(2) FMM_P(3) FMM_P(4) FMM_P(5) FMM_P(6) FMM_P(7) FMM_P(8) FMM_P(9) FMM_P(10)
+    FMM_P(11) FMM_P(12) FMM_P(13) FMM_P(14) FMM_P(15) FMM_P(16) FMM_P(17) FMM_P(18) FMM_P(19) FMM_P(20)
+#undef FMM_P
+    default:
+      throw Error{FMM_ERR_ARGUMENT, "expansion order out of range"};
+  }
 }
 
 __global__ void __launch_bounds__(32) k_op_p2m(const double4* __restrict__ pos, const double4* __restrict__ str,
@@ -736,13 +882,13 @@ void upload_tables(DevTables& dt, int p, cudaStream_t st) {
 
 void launch_p2m(DevTree& s, int p, int kind, const DevTables&, cudaStream_t st) {
   if (s.n_leaves == 0) return;
-  size_t sm = (size_t)kWarps * 2 * nh(p) * sizeof(double);
-  allow_smem(k_p2m, sm);
-  int g = (int)((s.n_leaves + kWarps - 1) / kWarps);
-  note_launch();
-  k_p2m<<<g, 32 * kWarps, sm, st>>>(s.leaf_index.ptr, (int)s.n_leaves, s.body_start.ptr, s.body_count.ptr,
-                                    s.scenter.ptr, s.pos.ptr, s.str.ptr, s.multipole.ptr, p, kind);
-  FMM_CUDA_TRY(cudaGetLastError());
+  if (kind == FMM_POINT_VORTEX) {
+    P2MLaneLaunch<true> f{s, st};
+    dispatch_order(p, f);
+  } else {
+    P2MLaneLaunch<false> f{s, st};
+    dispatch_order(p, f);
+  }
 }
 
 namespace {
