@@ -41,8 +41,11 @@ constexpr int kLenT = (kLaneMaxP + 1) * (kLaneMaxP + 2) * (2 * kLaneMaxP + 3) / 
 constexpr int kNhMax = (kLaneMaxP + 1) * (kLaneMaxP + 2) / 2;
 constexpr unsigned kAll = 0xffffffffu;
 
-// [lenT(n-1) + row (n+1) + nu]: zeta (multipole) and eta (local) magnitude sets
-__constant__ double c_HBz[kLenT], c_HAz[kLenT], c_HBe[kLenT], c_HAe[kLenT];
+// column nu of degree n at [lenT(n-1) + nu (n+1)]: B H over a, (A H w / 2) over m;
+// zeta (multipole) and eta (local) magnitude sets.  kLaneMaxP padding entries let
+// a sum run to the kernel's maximum order past the degree (its inputs are zero).
+constexpr int kLenTPad = kLenT + kLaneMaxP + 1;
+__constant__ double c_HBz[kLenTPad], c_HAz[kLenTPad], c_HBe[kLenTPad], c_HAe[kLenTPad];
 __constant__ double c_Mt[kNhMax], c_Lt[kNhMax];
 
 __host__ __device__ constexpr int hi(int n, int m) { return n * (n + 1) / 2 + m; }
@@ -59,7 +62,8 @@ void ensure_lane_tables(cudaStream_t st) {
   if (dev < 64 && g_tab_done[dev]) return;
   HostTables h;
   build_tables(h, kLaneMaxP);
-  std::vector<double> hbz(kLenT), haz(kLenT), hbe(kLenT), hae(kLenT), mt(kNhMax), lt(kNhMax);
+  std::vector<double> hbz(kLenTPad, 0.0), haz(kLenTPad, 0.0), hbe(kLenTPad, 0.0), hae(kLenTPad, 0.0), mt(kNhMax),
+      lt(kNhMax);
   for (int n = 0; n <= kLaneMaxP; ++n) {
     const double* H = h.Hs.data() + length_Hs(n - 1);
     const double* z = h.zeta.data() + length_Ts(n - 1);
@@ -69,31 +73,32 @@ void ensure_lane_tables(cudaStream_t st) {
       for (int nu = 0; nu <= n; ++nu) {
         const double Hv = H[H_index(std::min(a, nu), std::max(a, nu))];
         const double w = nu == 0 ? 0.5 : 1.0;
-        hbz[off + a * (n + 1) + nu] = z[a] * Hv;  // B(a): row 0 of the magnitudes
-        hbe[off + a * (n + 1) + nu] = e[a] * Hv;
-        haz[off + a * (n + 1) + nu] = z[a * (n + 1)] * Hv * w;  // A(m): column 0
-        hae[off + a * (n + 1) + nu] = e[a * (n + 1)] * Hv * w;
+        hbz[off + nu * (n + 1) + a] = z[a] * Hv;  // B(a): row 0 of the magnitudes
+        hbe[off + nu * (n + 1) + a] = e[a] * Hv;
+        haz[off + nu * (n + 1) + a] = z[a * (n + 1)] * Hv * w;  // A(m): column 0, m = a
+        hae[off + nu * (n + 1) + a] = e[a * (n + 1)] * Hv * w;
       }
   }
   for (int i = 0; i < kNhMax; ++i) {
     mt[i] = h.Mt[i];
     lt[i] = h.Lt[i];
   }
-  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBz, hbz.data(), kLenT * 8, 0, cudaMemcpyHostToDevice, st));
-  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAz, haz.data(), kLenT * 8, 0, cudaMemcpyHostToDevice, st));
-  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBe, hbe.data(), kLenT * 8, 0, cudaMemcpyHostToDevice, st));
-  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAe, hae.data(), kLenT * 8, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBz, hbz.data(), kLenTPad * 8, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAz, haz.data(), kLenTPad * 8, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBe, hbe.data(), kLenTPad * 8, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAe, hae.data(), kLenTPad * 8, 0, cudaMemcpyHostToDevice, st));
   FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Mt, mt.data(), kNhMax * 8, 0, cudaMemcpyHostToDevice, st));
   FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Lt, lt.data(), kNhMax * 8, 0, cudaMemcpyHostToDevice, st));
   FMM_CUDA_TRY(cudaStreamSynchronize(st));
   if (dev < 64) g_tab_done[dev] = true;
 }
 
-// rotate_y of degree n (X -> Y) on expansions padded to PMAX + 1 registers;
-// LOCAL: eta magnitudes and e^{-+i nu beta}.  The nu loop runs at run time
-// and fuses both matrix products (stage 2 accumulates P_nu +- Q_nu into every
-// output as soon as it is formed), so the code stays small; the unrolled a and
-// m loops are predicated at n (entries past n multiply zeros or are dropped).
+// rotate_y of degree n (X -> Y) on expansions padded to PMAX + 1 registers
+// (entries past n are zero); LOCAL: eta magnitudes and e^{-+i nu beta}.  The nu
+// loop runs at run time and fuses both matrix products: column nu of B H gives
+// E, O, Z, and P_nu +- Q_nu is accumulated into every output at once through
+// column nu of A H w / 2.  Sums run to PMAX from one column base, so the table
+// entries are uniform constant reads at fixed offsets and no term is predicated.
 template <int PMAX, bool LOCAL>
 __device__ __forceinline__ void rot_y(int n, const double (&Xr)[PMAX + 1], const double (&Xi)[PMAX + 1], double cb,
                                       double sb, double (&Yr)[PMAX + 1], double (&Yi)[PMAX + 1]) {
@@ -109,21 +114,20 @@ __device__ __forceinline__ void rot_y(int n, const double (&Xr)[PMAX + 1], const
       c = cn;
       s = sn;
     }
+    const int col = t0 + nu * w;
     double Er = 0, Ei = 0, Or = 0, Oi = 0;
 #pragma unroll
     for (int a = 1; a <= PMAX; ++a) {
-      if (a <= n) {
-        const double h = LOCAL ? c_HBe[t0 + a * w + nu] : c_HBz[t0 + a * w + nu];
-        if (a & 1) {
-          Or += h * Xr[a];
-          Oi += h * Xi[a];
-        } else {
-          Er += h * Xr[a];
-          Ei += h * Xi[a];
-        }
+      const double h = LOCAL ? c_HBe[col + a] : c_HBz[col + a];
+      if (a & 1) {
+        Or += h * Xr[a];
+        Oi += h * Xi[a];
+      } else {
+        Er += h * Xr[a];
+        Ei += h * Xi[a];
       }
     }
-    const double h0 = LOCAL ? c_HBe[t0 + nu] : c_HBz[t0 + nu];
+    const double h0 = LOCAL ? c_HBe[col] : c_HBz[col];
     const double Zr = h0 * Xr[0], Zi = h0 * Xi[0];
     const double sg = ((n + nu) & 1) ? -1.0 : 1.0;
     const double S1r = Er - Or, S1i = Ei - Oi;
@@ -138,11 +142,9 @@ __device__ __forceinline__ void rot_y(int n, const double (&Xr)[PMAX + 1], const
     const double Rpr = Pr + Qr, Rpi = Pi + Qi, Rmr = Pr - Qr, Rmi = Pi - Qi;
 #pragma unroll
     for (int m = 0; m <= PMAX; ++m) {
-      if (m <= n) {
-        const double h = LOCAL ? c_HAe[t0 + m * w + nu] : c_HAz[t0 + m * w + nu];
-        Yr[m] += h * ((m & 1) ? Rmr : Rpr);
-        Yi[m] += h * ((m & 1) ? Rmi : Rpi);
-      }
+      const double h = LOCAL ? c_HAe[col + m] : c_HAz[col + m];
+      Yr[m] += h * ((m & 1) ? Rmr : Rpr);
+      Yi[m] += h * ((m & 1) ? Rmi : Rpi);
     }
   }
 }
@@ -157,6 +159,7 @@ struct Pair {
   bool ok;      // tolerance met
   // error control (src/translate.jl:1124-1412, :555-829)
   double thr, r_mp_inv, r_mp_inv_np2, r_l, r_l_nm1, nm1_fact_inv, np1_fact, n_fact_t_np1, mp_phi, Mn0;
+  double un;  // n! / t^(n+1) of the current degree (coaxial factor of source degree 0)
 };
 
 // rotated multipole in shared memory: plane c (re, im) of coefficient i, column lane
@@ -198,28 +201,15 @@ __device__ __forceinline__ double fwd_degree(int n, const Pair& q, double* Ms, i
   return sqrt(pw);
 }
 
-// (n + m)! / t^(n + m + 1) by the reference's recurrence (src/translate.jl:184-225)
-__device__ __forceinline__ double coef0(int n, int m, double one_over_t) {
-  double c = one_over_t;
-#pragma unroll 1
-  for (int k = 0; k < n; ++k) c *= (k + 1) * one_over_t;
-  int nm = n;
-#pragma unroll 1
-  for (int j = 0; j < m; ++j) {
-    nm += 1;
-    c *= nm * one_over_t;
-  }
-  return c;
-}
-
 // local error estimate of degree n from the rotated multipole of degrees <= n
 __device__ __forceinline__ double eps_local(int n, const Pair& q, const double* Ms, int lane, bool power) {
   if (power) {
     // degree n of translate_multipole_to_local_z_n! and local_power (src/translate.jl:238-295, :455-502)
-    double a = 0.0;
+    double a = 0.0, cs = q.un;
 #pragma unroll 1
     for (int m = 0; m <= n; ++m) {
-      double c = coef0(n, m, q.rinv);
+      if (m > 0) cs *= (n + m) * q.rinv;  // (n + m)! / t^(n+m+1), the reference's product order
+      double c = cs;
       int n_np = n + m;
       double vr = 0, vi = 0;
 #pragma unroll 1
@@ -295,15 +285,17 @@ __device__ __forceinline__ void err_step(int n, Pair& q, const double* Ms, int l
 // (sources m..P), rotate_y back, back_rotate_z, then the sum over the 32 lanes
 // into the warp accumulator (stage: 2 (PMAX+1) rows of 33 doubles)
 template <int PMAX>
-__device__ __forceinline__ void back_degree(int n, const Pair& q, const double* Ms, double* stage, double* acc,
-                                            int lane) {
+__device__ __forceinline__ void back_degree(int n, double un, const Pair& q, const double* Ms, double* stage,
+                                            double* acc, int lane) {
   const bool on = q.valid && n <= q.P;
   double Xr[PMAX + 1], Xi[PMAX + 1];
+  double cs = un;
 #pragma unroll
   for (int m = 0; m <= PMAX; ++m) {
     Xr[m] = Xi[m] = 0.0;
     if (m > n) continue;
-    double c = coef0(n, m, q.rinv);
+    if (m > 0) cs *= (n + m) * q.rinv;  // (n + m)! / t^(n+m+1), the reference's product order
+    double c = cs;
     int n_np = n + m;
     double vr = 0, vi = 0;
     const int top = on ? q.P : m - 1;
@@ -411,6 +403,7 @@ __global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_lis
     q.sth = 0.0;
     q.r = 1.0;
     q.rinv = 1.0;
+    q.un = 1.0;
     if (q.valid) {
       const int s = src_of[l];
       q.src = multipole + (int64_t)4 * NH * s;
@@ -429,6 +422,7 @@ __global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_lis
         q.cth = (q.r > 0 && z < 0) ? -1.0 : 1.0;
       }
       q.rinv = 1 / q.r;
+      q.un = q.rinv;
       if (errc) {
         const double mdx = min_dist_1d(x, -tb0, tb0), mdy = min_dist_1d(y, -tb1, tb1), mdz = min_dist_1d(z, -tb2, tb2);
         const double r_mp = sqrt(mdx * mdx + mdy * mdy + mdz * mdz);
@@ -453,6 +447,7 @@ __global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_lis
     for (int n = 0; n <= PMAX; ++n) {
       if (!__any_sync(kAll, q.active)) break;
       if (!q.active) continue;
+      if (n > 0) q.un *= n * q.rinv;
       double y0r, y1r, y1i;
       const double pn_phi = fwd_degree<PMAX>(n, q, Ms, lane, y0r, y1r, y1i);
       if (errc && n > 0) err_step<PMAX>(n, q, Ms, lane, power, be, pn_phi, y0r, y1r, y1i);
@@ -462,8 +457,12 @@ __global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_lis
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) pw = max(pw, __shfl_xor_sync(kAll, pw, o));
     __syncwarp();
+    double un = q.rinv;
 #pragma unroll 1
-    for (int n = 0; n <= pw; ++n) back_degree<PMAX>(n, q, Ms, stage, acc, lane);
+    for (int n = 0; n <= pw; ++n) {
+      if (n > 0) un *= n * q.rinv;
+      back_degree<PMAX>(n, un, q, Ms, stage, acc, lane);
+    }
     if (q.valid) {
       if (p_used) p_used[l] = q.P;
       pmax = max(pmax, q.P);
