@@ -85,6 +85,11 @@ WORKLOADS = {
 }
 
 
+# DRAM bytes (read + write) of the solve's near-field launch, one ncu capture of the full-size
+# workload (dram__bytes_read.sum + dram__bytes_write.sum)
+NEAR_TRAFFIC = {"c2": 318682112 + 41943808}
+
+
 def options(fm, w, precision):
     err = fm.PowerRelativeGradient(w["err"]) if w["err"] else None
     return fm.make_options(expansion_order=w["p"], leaf_size_source=w["ls"], multipole_acceptance=w["mac"],
@@ -292,11 +297,17 @@ def gpu_arm(args, w, rank, world, local_rank):
     dom = max(("nearfield", "horizontal"), key=lambda k: stages[k])
     if dom == "nearfield":
         ach = near_flops / (stages["nearfield"] * 1e-3) / 1e12
+        traffic = NEAR_TRAFFIC.get(args.config) if not args.bodies else None
         roof = {"kernel": "k_p2p (FP32, mixed)", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": None,
+                "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": traffic,
                 "work": f"{st_mixed['n_p2p_pairs']:.3e} pairs x {w['flops_per_pair']} flop",
                 "peak_source": f"nominal FP32 CUDA-core peak, {sms} SMs x 128 lanes x 2 x {sm_max:.0f} MHz "
                                "(MEASURED_PEAKS.json holds no CUDA-core figure)"}
+        if traffic:
+            gbs = traffic / (stages["nearfield"] * 1e-3) / 1e9
+            roof["hbm_view"] = {"achieved_gbs": gbs, "peak_gbs": pk.get("hbm_gbs"),
+                                "frac": gbs / pk["hbm_gbs"] if pk.get("hbm_gbs") else None,
+                                "note": "DRAM bytes of one launch (ncu) over its event time: not HBM-bound"}
     else:
         ach = st_mixed["m2l_flops"] / (stages["horizontal"] * 1e-3) / 1e12
         roof = {"kernel": "k_m2l (FP64)", "bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
