@@ -100,6 +100,9 @@ void launch_m2m(DevTree& s, int p, bool lh, const DevTables& tb, cudaStream_t st
 // per-pair orders go to p_used (device, one per m2l entry) when non-null; stats (device,
 // 4 ints, zeroed by the caller) receives the max order, a failure flag and the flop count
 // lane-per-pair M2L (m2l_lane.cu): point sources, orders 1..12; false = not handled
+// lane-per-child M2M (orders 1..12) / L2L (orders 1..6), point sources (m2l_lane.cu); false = not handled
+bool launch_m2m_lane(DevTree& s, int p, bool lh, cudaStream_t st);
+bool launch_l2l_lane(DevTree& t, int p, bool lh, cudaStream_t st);
 bool launch_m2l_lane(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh, int em, double eps, int be,
                      int* p_used, int* stats, cudaStream_t st);
 void launch_m2l(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh, int error_method, double eps,

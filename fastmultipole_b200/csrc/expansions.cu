@@ -995,6 +995,7 @@ struct OpM2LLaunch {
 }  // namespace
 
 void launch_m2m(DevTree& s, int p, bool lh, const DevTables& tb, cudaStream_t st) {
+  if (launch_m2m_lane(s, p, lh, st)) return;
   M2MLaunch f{s, p, tab_of(tb), st};
   dispatch_slots(p, lh, f);
 }
@@ -1030,6 +1031,7 @@ void launch_m2l(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh,
 }
 
 void launch_l2l(DevTree& t, int p, bool lh, const DevTables& tb, cudaStream_t st) {
+  if (launch_l2l_lane(t, p, lh, st)) return;
   L2LLaunch f{t, p, tab_of(tb), st};
   dispatch_slots(p, lh, f);
 }

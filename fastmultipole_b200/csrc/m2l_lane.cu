@@ -500,6 +500,268 @@ void run_lane(DevTree& t, const DevTree& s, const DevLists& L, int em, double ep
   FMM_CUDA_TRY(cudaGetLastError());
 }
 
+// ---------------------------------------------------------------------------
+// M2M and L2L with one lane per child (multipole_to_multipole!, src/translate.jl:
+// 144-174; local_to_local!, :1896-1926): rotate_z -> rotate_y -> coaxial
+// translation (translate_multipole_z!, :6-50; translate_local_z!, :1851-1891) ->
+// rotate_y -> back_rotate_z, both rotations with the zeta set for M2M and the
+// eta set for L2L, as the reference's chain does.
+
+struct Geo {
+  double cph, sph, cth, sth, r;
+};
+// cartesian_to_spherical (src/rotate.jl:9-21) in cos/sin form
+__device__ __forceinline__ Geo geo_of(double x, double y, double z) {
+  Geo g{1.0, 0.0, 1.0, 0.0, 0.0};
+  const double x2y2 = x * x + y * y;
+  const double r2 = x2y2 + z * z;
+  g.r = (r2 == 0.0) ? r2 : sqrt(r2);
+  if (x2y2 > 0) {
+    const double rho = sqrt(x2y2);
+    g.cph = x / rho;
+    g.sph = y / rho;
+    g.cth = z / g.r;
+    g.sth = rho / g.r;
+  } else {
+    g.cth = (g.r > 0 && z < 0) ? -1.0 : 1.0;
+  }
+  return g;
+}
+
+// rotate_z of degree n of an interleaved expansion (set 0) into padded registers
+template <int PMAX>
+__device__ __forceinline__ void rotz_in(int n, bool on, const double* e, const Geo& g, double (&Xr)[PMAX + 1],
+                                        double (&Xi)[PMAX + 1]) {
+  double er = 1.0, ei = 0.0;
+  const int base = hi(n, 0);
+#pragma unroll
+  for (int a = 0; a <= PMAX; ++a) {
+    Xr[a] = Xi[a] = 0.0;
+    if (a > n || !on) continue;
+    const double2 u = __ldg(reinterpret_cast<const double2*>(e) + 2 * (base + a));
+    Xr[a] = n == 0 ? u.x : u.x * er - u.y * ei;
+    Xi[a] = n == 0 ? u.y : u.x * ei + u.y * er;
+    const double t = er;
+    er = er * g.cph - ei * g.sph;
+    ei = t * g.sph + ei * g.cph;
+  }
+}
+
+// back_rotate_z of degree n in place
+template <int PMAX>
+__device__ __forceinline__ void rotz_back(int n, const Geo& g, double (&Yr)[PMAX + 1], double (&Yi)[PMAX + 1]) {
+  double er = 1.0, ei = 0.0;
+#pragma unroll
+  for (int m = 0; m <= PMAX; ++m) {
+    if (m > n) break;
+    const double cr = er, ci = -ei;
+    const double vr = n == 0 ? Yr[m] : Yr[m] * cr - Yi[m] * ci;
+    const double vi = n == 0 ? Yi[m] : Yr[m] * ci + Yi[m] * cr;
+    Yr[m] = vr;
+    Yi[m] = vi;
+    const double t = er;
+    er = er * g.cph - ei * g.sph;
+    ei = t * g.sph + ei * g.cph;
+  }
+}
+
+// M2M of one level: warp w takes parents l0 + 4 w .. + 3; lanes 8 g .. 8 g + 7 carry
+// the children of parent l0 + 4 w + g; per degree the eight contributions are summed
+// by shuffles and added to the parent by the group's first lane
+template <int PMAX>
+__global__ void __launch_bounds__(32) k_m2m_lane(int l0, int l1, const int* __restrict__ child_start,
+                                                 const int* __restrict__ n_children,
+                                                 const double* __restrict__ scen, double* __restrict__ M) {
+  constexpr int NH = hi(PMAX + 1, 0);
+  extern __shared__ double lane_smem[];
+  double* Ms = lane_smem;  // [2 NH][32]
+  const int lane = threadIdx.x, j = lane & 7;
+  const int k = l0 + blockIdx.x * 4 + (lane >> 3);
+  bool on = false;
+  int c = 0;
+  if (k < l1 && j < n_children[k]) {
+    on = true;
+    c = child_start[k] + j;
+  }
+  Geo g{1.0, 0.0, 1.0, 0.0, 0.0};
+  if (on) g = geo_of(scen[3 * k] - scen[3 * c], scen[3 * k + 1] - scen[3 * c + 1], scen[3 * k + 2] - scen[3 * c + 2]);
+  const double* src = M + (int64_t)4 * NH * c;
+  double* dst = M + (int64_t)4 * NH * (k < l1 ? k : l0);
+  const double mt = -g.r;
+#pragma unroll 1
+  for (int n = 0; n <= PMAX; ++n) {
+    double Xr[PMAX + 1], Xi[PMAX + 1], Yr[PMAX + 1], Yi[PMAX + 1];
+    rotz_in<PMAX>(n, on, src, g, Xr, Xi);
+    rot_y<PMAX, false>(n, Xr, Xi, g.cth, g.sth, Yr, Yi);
+#pragma unroll
+    for (int m = 0; m <= PMAX; ++m) {
+      if (m > n) break;
+      MS(Ms, hi(n, m), 0, lane) = Yr[m];
+      MS(Ms, hi(n, m), 1, lane) = Yi[m];
+    }
+    // translate_multipole_z!: out(n, m) = sum_{n' = n..m} (-t)^(n-n') / (n-n')! M(n', m)
+#pragma unroll
+    for (int m = 0; m <= PMAX; ++m) {
+      Xr[m] = Xi[m] = 0.0;
+      if (m > n) continue;
+      double f = 1.0, tp = 1.0, vr = 0.0, vi = 0.0;
+      int q = 1;
+#pragma unroll 1
+      for (int np = n; np >= m; --np) {
+        const double cc = tp / f;
+        vr += cc * MSr(Ms, hi(np, m), 0, lane);
+        vi += cc * MSr(Ms, hi(np, m), 1, lane);
+        tp *= mt;
+        f *= q;
+        q += 1;
+      }
+      Xr[m] = vr;
+      Xi[m] = vi;
+    }
+    rot_y<PMAX, false>(n, Xr, Xi, g.cth, g.sth, Yr, Yi);
+    rotz_back<PMAX>(n, g, Yr, Yi);
+#pragma unroll
+    for (int m = 0; m <= PMAX; ++m) {
+      if (m > n) break;
+      double vr = on ? Yr[m] : 0.0, vi = on ? Yi[m] : 0.0;
+      vr += __shfl_xor_sync(kAll, vr, 1);
+      vi += __shfl_xor_sync(kAll, vi, 1);
+      vr += __shfl_xor_sync(kAll, vr, 2);
+      vi += __shfl_xor_sync(kAll, vi, 2);
+      vr += __shfl_xor_sync(kAll, vr, 4);
+      vi += __shfl_xor_sync(kAll, vi, 4);
+      if (j == 0 && k < l1 && n_children[k] > 0) {
+        dst[4 * hi(n, m)] += vr;
+        dst[4 * hi(n, m) + 1] += vi;
+      }
+    }
+  }
+}
+
+// L2L of one level: one lane per child c in [c0, c1), from its parent's local expansion
+template <int PMAX>
+__global__ void __launch_bounds__(32) k_l2l_lane(int c0, int c1, const int* __restrict__ parent,
+                                                 const double* __restrict__ tcen, double* __restrict__ L) {
+  constexpr int NH = hi(PMAX + 1, 0);
+  extern __shared__ double lane_smem[];
+  double* Ls = lane_smem;  // rotated parent local, [2 NH][32]
+  const int lane = threadIdx.x;
+  const int c = c0 + blockIdx.x * 32 + lane;
+  const bool on = c < c1;
+  int k = 0;
+  Geo g{1.0, 0.0, 1.0, 0.0, 0.0};
+  if (on) {
+    k = parent[c];
+    g = geo_of(tcen[3 * c] - tcen[3 * k], tcen[3 * c + 1] - tcen[3 * k + 1], tcen[3 * c + 2] - tcen[3 * k + 2]);
+  }
+  const double* src = L + (int64_t)4 * NH * k;
+  double* dst = L + (int64_t)4 * NH * (on ? c : c0);
+  const double mt = -g.r;
+#pragma unroll 1
+  for (int n = 0; n <= PMAX; ++n) {
+    double Xr[PMAX + 1], Xi[PMAX + 1], Yr[PMAX + 1], Yi[PMAX + 1];
+    rotz_in<PMAX>(n, on, src, g, Xr, Xi);
+    rot_y<PMAX, true>(n, Xr, Xi, g.cth, g.sth, Yr, Yi);
+#pragma unroll
+    for (int m = 0; m <= PMAX; ++m) {
+      if (m > n) break;
+      MS(Ls, hi(n, m), 0, lane) = Yr[m];
+      MS(Ls, hi(n, m), 1, lane) = Yi[m];
+    }
+  }
+#pragma unroll 1
+  for (int n = 0; n <= PMAX; ++n) {
+    // translate_local_z!: out(n, m) = sum_{n' = n..P} prod_{q=1}^{n'-n} (-t / q) L(n', m)
+    double Xr[PMAX + 1], Xi[PMAX + 1], Yr[PMAX + 1], Yi[PMAX + 1];
+#pragma unroll
+    for (int m = 0; m <= PMAX; ++m) {
+      Xr[m] = Xi[m] = 0.0;
+      if (m > n) continue;
+      double cc = 1.0, vr = 0.0, vi = 0.0;
+      int q = 1;
+#pragma unroll 1
+      for (int np = n; np <= PMAX; ++np) {
+        vr += cc * MSr(Ls, hi(np, m), 0, lane);
+        vi += cc * MSr(Ls, hi(np, m), 1, lane);
+        cc *= mt / q;
+        q += 1;
+      }
+      Xr[m] = vr;
+      Xi[m] = vi;
+    }
+    rot_y<PMAX, true>(n, Xr, Xi, g.cth, g.sth, Yr, Yi);
+    rotz_back<PMAX>(n, g, Yr, Yi);
+    if (on) {
+#pragma unroll
+      for (int m = 0; m <= PMAX; ++m) {
+        if (m > n) break;
+        dst[4 * hi(n, m)] += Yr[m];
+        dst[4 * hi(n, m) + 1] += Yi[m];
+      }
+    }
+  }
+}
+
+template <int PMAX>
+void run_m2m_lane(DevTree& s, cudaStream_t st) {
+  const size_t sm = (size_t)2 * hi(PMAX + 1, 0) * 32 * sizeof(double);
+  if (sm > 48 * 1024)
+    FMM_CUDA_TRY(cudaFuncSetAttribute(k_m2m_lane<PMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  for (int l = s.n_levels - 2; l >= 0; --l) {
+    const int l0 = (int)s.levels_start[l], l1 = (int)s.levels_end[l];
+    if (l1 <= l0) continue;
+    note_launch();
+    k_m2m_lane<PMAX><<<(l1 - l0 + 3) / 4, 32, sm, st>>>(l0, l1, s.child_start.ptr, s.n_children.ptr, s.scenter.ptr,
+                                                         s.multipole.ptr);
+  }
+  FMM_CUDA_TRY(cudaGetLastError());
+}
+
+template <int PMAX>
+void run_l2l_lane(DevTree& t, cudaStream_t st) {
+  const size_t sm = (size_t)2 * hi(PMAX + 1, 0) * 32 * sizeof(double);
+  if (sm > 48 * 1024)
+    FMM_CUDA_TRY(cudaFuncSetAttribute(k_l2l_lane<PMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  for (int l = 1; l < t.n_levels; ++l) {
+    const int c0 = (int)t.levels_start[l], c1 = (int)t.levels_end[l];
+    if (c1 <= c0) continue;
+    note_launch();
+    k_l2l_lane<PMAX><<<(c1 - c0 + 31) / 32, 32, sm, st>>>(c0, c1, t.parent.ptr, t.tcenter.ptr, t.local.ptr);
+  }
+  FMM_CUDA_TRY(cudaGetLastError());
+}
+
+template <class F>
+void lane_dispatch(int p, F&& f) {
+  switch (p) {
+    case 1: f.template go<1>(); break;
+    case 2: f.template go<2>(); break;
+    case 3: f.template go<3>(); break;
+    case 4: f.template go<4>(); break;
+    case 5: f.template go<5>(); break;
+    case 6: f.template go<6>(); break;
+    case 7: f.template go<7>(); break;
+    case 8: f.template go<8>(); break;
+    case 9: f.template go<9>(); break;
+    case 10: f.template go<10>(); break;
+    case 11: f.template go<11>(); break;
+    default: f.template go<12>(); break;
+  }
+}
+
+struct M2MLaneGo {
+  DevTree& s;
+  cudaStream_t st;
+  template <int P>
+  void go() { run_m2m_lane<P>(s, st); }
+};
+struct L2LLaneGo {
+  DevTree& t;
+  cudaStream_t st;
+  template <int P>
+  void go() { run_l2l_lane<P>(t, st); }
+};
+
 }  // namespace
 
 bool launch_m2l_lane(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh, int em, double eps, int be,
@@ -521,6 +783,27 @@ bool launch_m2l_lane(DevTree& t, const DevTree& s, const DevLists& L, int p, boo
     case 11: run_lane<11>(t, s, L, em, eps, be, p_used, stats, st); break;
     default: run_lane<12>(t, s, L, em, eps, be, p_used, stats, st); break;
   }
+  return true;
+}
+
+}  // namespace fmmb
+
+namespace fmmb {
+
+bool launch_m2m_lane(DevTree& s, int p, bool lh, cudaStream_t st) {
+  if (lh || p < 1 || p > kLaneMaxP) return false;
+  if (s.n_levels < 2) return true;
+  ensure_lane_tables(st);
+  lane_dispatch(p, M2MLaneGo{s, st});
+  return true;
+}
+
+bool launch_l2l_lane(DevTree& t, int p, bool lh, cudaStream_t st) {
+  // above order 6 the warp-per-child engine is faster (one rotation pair per child, no reduction)
+  if (lh || p < 1 || p > 6) return false;
+  if (t.n_levels < 2) return true;
+  ensure_lane_tables(st);
+  lane_dispatch(p, L2LLaneGo{t, st});
   return true;
 }
 
