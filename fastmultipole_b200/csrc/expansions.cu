@@ -1005,7 +1005,7 @@ void launch_m2l(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh,
   if (L.n_m2l_targets == 0) return;
   // stats: [0] = max order used, [1] = any tolerance missed, [2..3] = flop count (u64)
   M2LStats S{stats, stats + 1, reinterpret_cast<unsigned long long*>(stats + 2)};
-  if (em == FMM_ERROR_NONE && p >= 1 && p <= 3) {
+  if (lh && em == FMM_ERROR_NONE && p >= 1 && p <= 3) {
     int g = (int)((L.n_m2l_targets + kWarps - 1) / kWarps);
     Tab T = tab_of(tb);
     note_launch();

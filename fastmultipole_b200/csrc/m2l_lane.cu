@@ -702,6 +702,106 @@ __global__ void __launch_bounds__(32) k_l2l_lane(int c0, int c1, const int* __re
   }
 }
 
+// Plain M2L at orders <= 3 (the influence estimate runs at order 3): one warp per
+// target, one lane per pair, the whole rotated multipole and the lane's share of
+// the target's local expansion in registers (every degree loop unrolled), the 32
+// shares summed by shuffles once per target.
+template <int P>
+__global__ void __launch_bounds__(128) k_m2l_small(const int* __restrict__ tgt_list, const int* __restrict__ off,
+                                                   const int* __restrict__ src_of, int n_targets,
+                                                   double* __restrict__ local, const double* __restrict__ multipole,
+                                                   const double* __restrict__ tcen, const double* __restrict__ scen,
+                                                   int* __restrict__ p_used, int* __restrict__ st_pmax,
+                                                   unsigned long long* __restrict__ st_flops) {
+  constexpr int NH = hi(P + 1, 0);
+  const int lane = threadIdx.x & 31;
+  const int b = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (b >= n_targets) return;
+  const int t = tgt_list[b];
+  const double tc0 = tcen[3 * t], tc1 = tcen[3 * t + 1], tc2 = tcen[3 * t + 2];
+  double accr[NH], acci[NH];
+#pragma unroll
+  for (int i = 0; i < NH; ++i) accr[i] = acci[i] = 0.0;
+  const int l0 = off[b], l1 = off[b + 1];
+  for (int l = l0 + lane; l < l1; l += 32) {
+    const int s = src_of[l];
+    const double* src = multipole + (int64_t)4 * NH * s;
+    const Geo g = geo_of(tc0 - scen[3 * s], tc1 - scen[3 * s + 1], tc2 - scen[3 * s + 2]);
+    const double rinv = 1 / g.r;
+    double Mr[NH], Mi[NH];
+#pragma unroll
+    for (int n = 0; n <= P; ++n) {
+      double Xr[P + 1], Xi[P + 1], Yr[P + 1], Yi[P + 1];
+      rotz_in<P>(n, true, src, g, Xr, Xi);
+      rot_y<P, false>(n, Xr, Xi, g.cth, g.sth, Yr, Yi);
+#pragma unroll
+      for (int m = 0; m <= n; ++m) {
+        Mr[hi(n, m)] = Yr[m];
+        Mi[hi(n, m)] = Yi[m];
+      }
+    }
+    double un = rinv;  // n! / t^(n+1), the reference's product order
+#pragma unroll
+    for (int n = 0; n <= P; ++n) {
+      if (n > 0) un *= n * rinv;
+      double Xr[P + 1], Xi[P + 1], Yr[P + 1], Yi[P + 1];
+      double cs = un;
+#pragma unroll
+      for (int m = 0; m <= P; ++m) {
+        Xr[m] = Xi[m] = 0.0;
+        if (m > n) continue;
+        if (m > 0) cs *= (n + m) * rinv;
+        double c = cs, vr = 0.0, vi = 0.0;
+        int n_np = n + m;
+#pragma unroll
+        for (int np = m; np <= P; ++np) {
+          vr += c * Mr[hi(np, m)];
+          vi += c * Mi[hi(np, m)];
+          n_np += 1;
+          c *= n_np * rinv;
+        }
+        Xr[m] = vr;
+        Xi[m] = vi;
+      }
+      rot_y<P, true>(n, Xr, Xi, g.cth, g.sth, Yr, Yi);
+      rotz_back<P>(n, g, Yr, Yi);
+#pragma unroll
+      for (int m = 0; m <= n; ++m) {
+        accr[hi(n, m)] += Yr[m];
+        acci[hi(n, m)] += Yi[m];
+      }
+    }
+    if (p_used) p_used[l] = P;
+  }
+#pragma unroll
+  for (int i = 0; i < NH; ++i)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      accr[i] += __shfl_xor_sync(kAll, accr[i], o);
+      acci[i] += __shfl_xor_sync(kAll, acci[i], o);
+    }
+  double* dst = local + (int64_t)4 * NH * t;
+#pragma unroll
+  for (int i = 0; i < NH; ++i)
+    if ((i & 31) == lane) {
+      dst[4 * i] += accr[i];
+      dst[4 * i + 1] += acci[i];
+    }
+  if (lane == 0) {
+    atomicMax(st_pmax, P);
+    atomicAdd(st_flops, (unsigned long long)(l1 - l0) * lane_pair_flops(P));
+  }
+}
+
+template <int P>
+void run_m2l_small(DevTree& t, const DevTree& s, const DevLists& L, int* p_used, int* stats, cudaStream_t st) {
+  note_launch();
+  k_m2l_small<P><<<(int)((L.n_m2l_targets + 3) / 4), 128, 0, st>>>(
+      L.m2l_tgt.ptr, L.m2l_off.ptr, L.m2l_s.ptr, (int)L.n_m2l_targets, t.local.ptr, s.multipole.ptr, t.tcenter.ptr,
+      s.scenter.ptr, p_used, stats, reinterpret_cast<unsigned long long*>(stats + 2));
+  FMM_CUDA_TRY(cudaGetLastError());
+}
+
 template <int PMAX>
 void run_m2m_lane(DevTree& s, cudaStream_t st) {
   const size_t sm = (size_t)2 * hi(PMAX + 1, 0) * 32 * sizeof(double);
@@ -769,6 +869,15 @@ bool launch_m2l_lane(DevTree& t, const DevTree& s, const DevLists& L, int p, boo
   if (lh || p < 1 || p > kLaneMaxP) return false;
   if (L.n_m2l_targets == 0) return true;
   ensure_lane_tables(st);
+  if (em == FMM_ERROR_NONE && p <= 3) {
+    if (p == 1)
+      run_m2l_small<1>(t, s, L, p_used, stats, st);
+    else if (p == 2)
+      run_m2l_small<2>(t, s, L, p_used, stats, st);
+    else
+      run_m2l_small<3>(t, s, L, p_used, stats, st);
+    return true;
+  }
   switch (p) {
     case 1: run_lane<1>(t, s, L, em, eps, be, p_used, stats, st); break;
     case 2: run_lane<2>(t, s, L, em, eps, be, p_used, stats, st); break;
