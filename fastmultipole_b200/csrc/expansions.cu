@@ -25,6 +25,7 @@ namespace {
 
 constexpr int kWarps = 4;                      // warps per CTA
 constexpr int kSlots = (231 + 31) / 32;        // nh(kMaxP) coefficients over 32 lanes
+__host__ __device__ constexpr int hi_nm(int n, int m) { return n * (n + 1) / 2 + m; }
 
 using eng::nm_of;
 using eng::sph;
@@ -409,13 +410,14 @@ __device__ __forceinline__ void p2m_body(double (&acc)[kSlots][4], double* h, in
   __syncwarp();
 }
 
-// P2M, one warp per leaf and one lane per body (32 bodies at a time): each lane
-// runs the regular-harmonic recurrence of calculate_q! (src/bodytomultipole.jl:
-// 112-139) for its body, degree n from degree n-1 in registers, forms the
-// degree-n contributions of body_to_multipole! (source: :283-334, vortex:
-// :387-489), and the 32 lanes' contributions are summed column by column through
-// shared memory into the leaf's multipole (the warp owns the leaf: no atomics).
-template <int PMAX, bool VORTEX>
+// P2M, one group of G lanes per leaf and one lane per body (G bodies at a time):
+// each lane runs the regular-harmonic recurrence of calculate_q!
+// (src/bodytomultipole.jl:112-139) for its body, degree n from degree n-1 in
+// registers, forms the degree-n contributions of body_to_multipole! (source:
+// :283-334, vortex: :387-489), and the group's contributions are summed into the
+// leaf's multipole (the group owns the leaf: no atomics) -- column by column
+// through shared memory for G = 32, by shuffles for G = 8 (leaves of a few bodies).
+template <int PMAX, bool VORTEX, int G>
 __global__ void __launch_bounds__(32 * kWarps) k_p2m_lane(const int* __restrict__ leaf_index, int n_leaves,
                                                           const int* __restrict__ body_start,
                                                           const int* __restrict__ body_count,
@@ -425,16 +427,19 @@ __global__ void __launch_bounds__(32 * kWarps) k_p2m_lane(const int* __restrict_
   constexpr int NC = VORTEX ? 4 : 2;  // doubles per coefficient written
   constexpr int ROWS = NC * (PMAX + 1);
   extern __shared__ double smem[];
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int w = blockIdx.x * kWarps + wid;
-  if (w >= n_leaves) return;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, gl = lane % G;
+  const int w = (blockIdx.x * kWarps + wid) * (32 / G) + lane / G;
+  if ((blockIdx.x * kWarps + wid) * (32 / G) >= n_leaves) return;  // the whole warp is past the end
   double* stage = smem + wid * ROWS * 33;
-  const int b = leaf_index[w];
-  const int s0 = body_start[b], cnt = body_count[b];
+  const bool has = w < n_leaves;
+  const int b = has ? leaf_index[w] : 0;
+  const int s0 = has ? body_start[b] : 0, cnt = has ? body_count[b] : 0;
   const double cx = scen[3 * b], cy = scen[3 * b + 1], cz = scen[3 * b + 2];
   double* Mb = M + (int64_t)4 * ((PMAX + 1) * (PMAX + 2) / 2) * b;
-  for (int j0 = 0; j0 < cnt; j0 += 32) {
-    const int j = j0 + lane;
+  int cmax = cnt;  // every lane runs the same number of batches (the reductions are warp-wide)
+  for (int o = 16; o > 0; o >>= 1) cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+  for (int j0 = 0; j0 < cmax; j0 += G) {
+    const int j = j0 + gl;
     const bool valid = j < cnt;
     double dx = 0, dy = 0, dz = 0;
     double4 sv = make_double4(0, 0, 0, 0);
@@ -523,22 +528,34 @@ __global__ void __launch_bounds__(32 * kWarps) k_p2m_lane(const int* __restrict_
             v3 = -(_1_m * _1_over_n * (0.5 * (vy * r1 - vx * r0 - vy * r5 - vx * r4) + vz * r3));
           }
         }
-        stage[(NC * m) * 33 + lane] = valid ? v0 : 0.0;
-        stage[(NC * m + 1) * 33 + lane] = valid ? v1 : 0.0;
-        if (VORTEX) {
-          stage[((NC * m + 2) % ROWS) * 33 + lane] = valid ? v2 : 0.0;
-          stage[((NC * m + 3) % ROWS) * 33 + lane] = valid ? v3 : 0.0;
+        if constexpr (G == 32) {
+          stage[(NC * m) * 33 + lane] = valid ? v0 : 0.0;
+          stage[(NC * m + 1) * 33 + lane] = valid ? v1 : 0.0;
+          if (VORTEX) {
+            stage[((NC * m + 2) % ROWS) * 33 + lane] = valid ? v2 : 0.0;
+            stage[((NC * m + 3) % ROWS) * 33 + lane] = valid ? v3 : 0.0;
+          }
+        } else {
+          double u[4] = {valid ? v0 : 0.0, valid ? v1 : 0.0, valid ? v2 : 0.0, valid ? v3 : 0.0};
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+#pragma unroll
+            for (int o = 1; o < G; o <<= 1) u[c] += __shfl_xor_sync(0xffffffffu, u[c], o);
+            if (gl == 0 && has) Mb[4 * hi_nm(n, m) + c] += u[c];
+          }
         }
       }
-      __syncwarp();
-      const int hn = n * (n + 1) / 2;
-      for (int v = lane; v < NC * (n + 1); v += 32) {
-        double t = 0.0;
+      if constexpr (G == 32) {
+        __syncwarp();
+        const int hn = n * (n + 1) / 2;
+        for (int v = lane; v < NC * (n + 1); v += 32) {
+          double t = 0.0;
 #pragma unroll 8
-        for (int k = 0; k < 32; ++k) t += stage[v * 33 + k];
-        Mb[4 * (hn + v / NC) + v % NC] += t;
+          for (int k = 0; k < 32; ++k) t += stage[v * 33 + k];
+          Mb[4 * (hn + v / NC) + v % NC] += t;
+        }
+        __syncwarp();
       }
-      __syncwarp();
     }
   }
 }
@@ -547,18 +564,27 @@ template <bool VORTEX>
 struct P2MLaneLaunch {
   DevTree& s;
   cudaStream_t st;
+  template <int PMAX, int G>
+  void run() {
+    constexpr size_t sm = G == 32 ? (size_t)kWarps * (VORTEX ? 4 : 2) * (PMAX + 1) * 33 * sizeof(double) : 0;
+    if (sm > 48 * 1024)
+      FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_lane<PMAX, VORTEX, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sm));
+    const int64_t per_cta = (int64_t)kWarps * (32 / G);
+    int g = (int)((s.n_leaves + per_cta - 1) / per_cta);
+    note_launch();
+    k_p2m_lane<PMAX, VORTEX, G><<<g, 32 * kWarps, sm, st>>>(s.leaf_index.ptr, (int)s.n_leaves, s.body_start.ptr,
+                                                              s.body_count.ptr, s.scenter.ptr, s.pos.ptr, s.str.ptr,
+                                                              s.multipole.ptr);
+    FMM_CUDA_TRY(cudaGetLastError());
+  }
   template <int PMAX>
   void go() {
-    constexpr size_t sm = (size_t)kWarps * (VORTEX ? 4 : 2) * (PMAX + 1) * 33 * sizeof(double);
-    if (sm > 48 * 1024)
-      FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_lane<PMAX, VORTEX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)sm));
-    int g = (int)((s.n_leaves + kWarps - 1) / kWarps);
-    note_launch();
-    k_p2m_lane<PMAX, VORTEX><<<g, 32 * kWarps, sm, st>>>(s.leaf_index.ptr, (int)s.n_leaves, s.body_start.ptr,
-                                                           s.body_count.ptr, s.scenter.ptr, s.pos.ptr, s.str.ptr,
-                                                           s.multipole.ptr);
-    FMM_CUDA_TRY(cudaGetLastError());
+    // leaves of a few bodies (on average <= 8) take groups of 8 lanes, four leaves per warp
+    if (s.n_bodies <= 8 * s.n_leaves)
+      run<PMAX, 8>();
+    else
+      run<PMAX, 32>();
   }
 };
 
@@ -1041,7 +1067,9 @@ void launch_l2p(DevTree& t, int p, bool lh, bool ps, bool gs, bool hs, double* a
   size_t sm = l2p_smem(p);
   allow_smem(k_l2p, sm);
   note_launch();
-  k_l2p<<<(int)t.n_leaves, kL2PThreads, sm, st>>>(t.leaf_index.ptr, t.body_start.ptr, t.body_count.ptr,
+  // leaves of a few bodies (on average <= 8) take one warp each instead of kL2PThreads threads
+  const int threads = t.n_bodies <= 8 * t.n_leaves ? 32 : kL2PThreads;
+  k_l2p<<<(int)t.n_leaves, threads, sm, st>>>(t.leaf_index.ptr, t.body_start.ptr, t.body_count.ptr,
                                                    t.tcenter.ptr, t.pos.ptr, t.local.ptr, p, lh ? 1 : 0,
                                                    ps ? 1 : 0, gs ? 1 : 0, hs ? 1 : 0, acc13);
   FMM_CUDA_TRY(cudaGetLastError());
