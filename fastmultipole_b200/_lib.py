@@ -84,6 +84,8 @@ SIGNATURES = {
                             C.POINTER(Result)]),
     "fmm_direct": (C.c_int, [C.c_void_p, C.POINTER(TargetSystem), C.POINTER(SourceSystem), C.c_int, C.c_int,
                              C.c_int, C.c_int]),
+    "fmm_vjp": (C.c_int, [C.c_void_p, C.POINTER(TargetSystem), C.POINTER(SourceSystem), C.POINTER(Options), _dp, _dp,
+                          _dp, _dp, C.POINTER(Result)]),
     "fmm_direct_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.POINTER(TargetSystem), C.POINTER(SourceSystem), C.c_int,
                                      C.c_int, C.c_int, C.c_int]),
     "fmm_get_tree": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TreeView)]),

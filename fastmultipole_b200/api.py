@@ -362,6 +362,69 @@ def solve_buffers(source_buf, kind, opt, target_pos=None, ctx=None, timing=False
     return out, res
 
 
+def vjp_buffers(source_buf, kind, opt, d_out, target_pos=None, ctx=None):
+    """Gradients of a loss through fmm! on raw buffers (fmm_vjp).
+
+    ``d_out`` (Nt, 16) holds dL/d(target buffer): column 3 (phi) for point sources,
+    columns 4..6 (velocity) for vortex particles.  Returns ``(out, d_strength,
+    d_source_position, d_target_position, fmm_result)``: the forward target buffer,
+    dL/dstrength (N,) or (N, 3), dL/dx (N, 3) and, for separate targets, dL/dy
+    (Nt, 3) (None when the sources are the targets)."""
+    ctx = ctx or default_context()
+    sb = np.ascontiguousarray(source_buf, dtype=np.float64)
+    n_s, d = sb.shape
+    src = L.SourceSystem(kind, n_s, d, sb.ctypes.data, L.FMM_MEMORY_HOST)
+    sdim = 1 if kind == L.FMM_POINT_SOURCE else 3
+    if target_pos is None:
+        nt = n_s
+        out = np.zeros((nt, 16))
+        tgt = L.TargetSystem(nt, None, 0, out.ctypes.data, L.FMM_MEMORY_HOST)
+        dtp = None
+    else:
+        tp = np.ascontiguousarray(target_pos, dtype=np.float64)
+        nt = len(tp)
+        out = np.zeros((nt, 16))
+        tgt = L.TargetSystem(nt, tp.ctypes.data, 3, out.ctypes.data, L.FMM_MEMORY_HOST)
+        dtp = np.zeros((nt, 3))
+    dd = np.ascontiguousarray(d_out, dtype=np.float64).reshape(nt, 16)
+    dstr = np.zeros((n_s, sdim))
+    dpos = np.zeros((n_s, 3))
+    res = L.Result()
+    ctx.check(L.lib().fmm_vjp(ctx.handle, C.byref(tgt), C.byref(src), C.byref(opt), dd.ctypes.data_as(L._dp),
+                              dstr.ctypes.data_as(L._dp), dpos.ctypes.data_as(L._dp),
+                              None if dtp is None else dtp.ctypes.data_as(L._dp), C.byref(res)))
+    return out, (dstr[:, 0] if sdim == 1 else dstr), dpos, dtp, res
+
+
+def vjp(system, d_potential=None, d_velocity=None, targets=None, *, leaf_size=20, expansion_order=5,
+        multipole_acceptance=0.4, error_tolerance=None, precision="f64", context=None):
+    """Gradient of L = sum_t d_potential_t phi_t (point sources) or sum_t d_velocity_t . u_t
+    (vortex particles) with respect to the source strengths and positions, and the
+    target positions when ``targets`` (a ProbeSystem or positions) is given.
+
+    The reference differentiates fmm! with ReverseDiff (README.md:19); this is the
+    adjoint FMM of the same problem.  Returns a dict with ``d_strength``,
+    ``d_position`` and (separate targets) ``d_target_position``."""
+    kind = _kind((system,))
+    buf = _source_buffer((system,), kind)
+    tpos = None
+    if targets is not None:
+        tpos = targets.positions() if hasattr(targets, "positions") else np.asarray(targets, dtype=np.float64)
+    nt = len(buf) if tpos is None else len(tpos)
+    d_out = np.zeros((nt, 16))
+    if kind == L.FMM_POINT_SOURCE:
+        d_out[:, 3] = np.asarray(d_potential, dtype=np.float64).reshape(nt)
+    else:
+        d_out[:, 4:7] = np.asarray(d_velocity, dtype=np.float64).reshape(nt, 3)
+    opt = make_options(expansion_order, leaf_size, None, multipole_acceptance, error_tolerance,
+                       scalar_potential=True, gradient=True, precision=precision)
+    out, dstr, dpos, dtp, res = vjp_buffers(buf, kind, opt, d_out, tpos, context)
+    r = {"d_strength": dstr, "d_position": dpos, "out": out, "error_success": bool(res.error_success)}
+    if dtp is not None:
+        r["d_target_position"] = dtp
+    return r
+
+
 def fmm(target_systems, source_systems=None, *, leaf_size=None, leaf_size_source=None, leaf_size_target=None,
         expansion_order=5, multipole_acceptance=0.4, error_tolerance=None, shrink_recenter=True,
         interaction_list_method=None, scalar_potential=False, gradient=True, hessian=False, farfield=True,

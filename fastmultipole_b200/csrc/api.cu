@@ -42,6 +42,74 @@ __global__ void k_unsort(const double* __restrict__ acc13, const int* __restrict
 
 int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); }
 
+// adjoint sources: at the targets (or the sources themselves), strengths = cotangents
+__global__ void k_adj_sources(int64_t n, const double* __restrict__ pos, int64_t stride, bool radius_from_pos,
+                              const double* __restrict__ dout16, int kind, double* __restrict__ buf) {
+  const int d = kind == FMM_POINT_SOURCE ? 5 : 7;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double* b = buf + d * i;
+    const double* x = pos + stride * i;
+    b[0] = x[0];
+    b[1] = x[1];
+    b[2] = x[2];
+    b[3] = radius_from_pos ? x[3] : 0.0;
+    if (kind == FMM_POINT_SOURCE) {
+      b[4] = dout16[16 * i + 3];
+    } else {
+      b[4] = dout16[16 * i + 4];
+      b[5] = dout16[16 * i + 5];
+      b[6] = dout16[16 * i + 6];
+    }
+  }
+}
+
+// dL/dstrength and dL/dx at the sources from the adjoint solve (adj16, at the sources)
+// and, when the sources are the targets, the forward solve and the cotangents
+__global__ void k_vjp_sources(int64_t n, int kind, const double* __restrict__ src, int d,
+                              const double* __restrict__ adj16, const double* __restrict__ fwd16,
+                              const double* __restrict__ dout16, double* __restrict__ dstr,
+                              double* __restrict__ dpos) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double* a = adj16 + 16 * i;
+    if (kind == FMM_POINT_SOURCE) {
+      const double q = src[d * i + 4];
+      dstr[i] = a[3];
+      for (int k = 0; k < 3; ++k) {
+        double v = -q * a[4 + k];
+        if (fwd16) v -= dout16[16 * i + 3] * fwd16[16 * i + 4 + k];
+        dpos[3 * i + k] = v;
+      }
+    } else {
+      const double* G = src + d * i + 4;
+      for (int c = 0; c < 3; ++c) dstr[3 * i + c] = a[4 + c];
+      for (int k = 0; k < 3; ++k) {
+        double v = 0.0;
+        for (int c = 0; c < 3; ++c) v += G[c] * a[7 + c + 3 * k];
+        if (fwd16)
+          for (int c = 0; c < 3; ++c) v += dout16[16 * i + 4 + c] * fwd16[16 * i + 7 + c + 3 * k];
+        dpos[3 * i + k] = v;
+      }
+    }
+  }
+}
+
+// dL/dy at a separate target system, from the forward solve
+__global__ void k_vjp_targets(int64_t n, int kind, const double* __restrict__ fwd16, const double* __restrict__ dout16,
+                              double* __restrict__ dtp) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double* f = fwd16 + 16 * i;
+    const double* w = dout16 + 16 * i;
+    for (int k = 0; k < 3; ++k) {
+      double v = 0.0;
+      if (kind == FMM_POINT_SOURCE)
+        v = -w[3] * f[4 + k];
+      else
+        for (int c = 0; c < 3; ++c) v += w[4 + c] * f[7 + c + 3 * k];
+      dtp[3 * i + k] = v;
+    }
+  }
+}
+
 }  // namespace
 
 struct fmm_ctx {
@@ -54,6 +122,7 @@ struct fmm_ctx {
   Scratch sc;
   DevTables tables;
   DevBuf<double> stage_s, stage_t, out16, est_out16;
+  DevBuf<double> adj_src, adj_out16, stage_d, vjp_out;  // fmm_vjp
   DevBuf<int> stats;
   bool have_solve = false;
   int last_p = 0;
@@ -343,6 +412,10 @@ int fmm_ctx_destroy(fmm_ctx* c) {
   c->stage_t.release();
   c->out16.release();
   c->est_out16.release();
+  c->adj_src.release();
+  c->adj_out16.release();
+  c->stage_d.release();
+  c->vjp_out.release();
   c->stats.release();
   delete c;
   return FMM_OK;
@@ -377,6 +450,7 @@ size_t fmm_ctx_device_bytes(const fmm_ctx* c) {
        (s.vals_a.cap + s.vals_b.cap + s.tmp_i.cap + s.tmp_j.cap + s.tmp_k.cap + s.cnt_a.cap + s.cnt_b.cap) * 4 +
        (s.front_a.cap + s.front_b.cap + s.dir_raw.cap + s.m2l_raw.cap) * 8 + s.tmp_d.cap * 8;
   b += (c->stage_s.cap + c->stage_t.cap + c->out16.cap + c->est_out16.cap) * 8;
+  b += (c->adj_src.cap + c->adj_out16.cap + c->stage_d.cap + c->vjp_out.cap) * 8;
   return b;
 }
 
@@ -438,6 +512,95 @@ int fmm_solve(fmm_ctx* c, const fmm_target_system* target, const fmm_source_syst
     c->have_solve = true;
     c->last_p = opt->expansion_order;
     c->last_kind = source->kind;
+    return FMM_OK;
+  } catch (const Error& e) {
+    return fail(c, e);
+  }
+}
+
+int fmm_vjp(fmm_ctx* c, const fmm_target_system* target, const fmm_source_system* source, const fmm_options* opt,
+            const double* d_out, double* d_strength, double* d_source_position, double* d_target_position,
+            fmm_result* result) {
+  if (!c) return FMM_ERR_ARGUMENT;
+  try {
+    FMM_CHECK(opt != nullptr, FMM_ERR_ARGUMENT, "options are NULL");
+    check_options(*opt);
+    check_source(source);
+    FMM_CHECK(target != nullptr, FMM_ERR_ARGUMENT, "target system is NULL (it carries the forward output)");
+    const bool self = target->positions == nullptr;
+    FMM_CHECK(self || target->stride >= 3, FMM_ERR_ARGUMENT, "target stride must be >= 3");
+    const int64_t ns = source->n_bodies, nt = self ? source->n_bodies : target->n_bodies;
+    FMM_CHECK(ns > 0 && nt > 0, FMM_ERR_ARGUMENT, "fmm_vjp needs sources and targets");
+    FMM_CHECK(target->out && d_out && d_strength && d_source_position, FMM_ERR_ARGUMENT,
+              "fmm_vjp: target->out, d_out, d_strength and d_source_position are required");
+    FMM_CHECK(target->memory == source->memory, FMM_ERR_ARGUMENT, "fmm_vjp: source and target memory must agree");
+    const int mem = source->memory;
+    FMM_CUDA_TRY(cudaSetDevice(c->device));
+    if (result) std::memset(result, 0, sizeof(*result));
+    const int kind = source->kind, d = source->data_per_body, sdim = kind == FMM_POINT_SOURCE ? 1 : 3;
+    c->have_solve = false;
+    // forward solve (the reference's fmm!): potential and gradient (point sources), velocity and its
+    // gradient (vortex particles)
+    fmm_options of = *opt;
+    of.scalar_potential = kind == FMM_POINT_SOURCE ? 1 : of.scalar_potential;
+    of.gradient = 1;
+    of.hessian = kind == FMM_POINT_VORTEX ? 1 : of.hessian;
+    SolveIn in;
+    in.d = d;
+    in.kind = kind;
+    in.n_s = ns;
+    in.n_t = nt;
+    in.src = stage(c, c->stage_s, source->buffer, (size_t)d * ns, mem);
+    in.tpos = nullptr;
+    in.t_stride = 0;
+    if (!self) {
+      in.tpos = stage(c, c->stage_t, target->positions, (size_t)target->stride * nt, mem);
+      in.t_stride = target->stride;
+    }
+    const double* dout = stage(c, c->stage_d, d_out, 16 * (size_t)nt, mem);
+    c->out16.grow(16 * (size_t)nt);
+    run_fmm(c, c->main, in, of, c->out16.ptr, result, false);
+    // adjoint solve: sources at the targets with the cotangents as strengths, targets at the sources
+    const int da = kind == FMM_POINT_SOURCE ? 5 : 7;
+    c->adj_src.grow((size_t)da * nt);
+    note_launch();
+    k_adj_sources<<<grid_for(nt), 256, 0, c->stream>>>(nt, self ? in.src : in.tpos, self ? d : in.t_stride, self,
+                                                        dout, kind, c->adj_src.ptr);
+    FMM_CUDA_TRY(cudaGetLastError());
+    SolveIn ia;
+    ia.d = da;
+    ia.kind = kind;
+    ia.n_s = nt;
+    ia.n_t = ns;
+    ia.src = c->adj_src.ptr;
+    ia.tpos = self ? nullptr : in.src;
+    ia.t_stride = self ? 0 : d;
+    fmm_options oa = of;
+    c->adj_out16.grow(16 * (size_t)ns);
+    run_fmm(c, c->main, ia, oa, c->adj_out16.ptr, nullptr, false);
+    // combine
+    const size_t n_res = (size_t)sdim * ns + 3 * (size_t)ns + (self ? 0 : 3 * (size_t)nt);
+    c->vjp_out.grow(n_res);
+    double* r_str = c->vjp_out.ptr;
+    double* r_pos = r_str + (size_t)sdim * ns;
+    double* r_tpos = r_pos + 3 * (size_t)ns;
+    note_launch();
+    k_vjp_sources<<<grid_for(ns), 256, 0, c->stream>>>(ns, kind, in.src, d, c->adj_out16.ptr,
+                                                        self ? c->out16.ptr : nullptr, self ? dout : nullptr, r_str,
+                                                        r_pos);
+    FMM_CUDA_TRY(cudaGetLastError());
+    if (!self) {
+      note_launch();
+      k_vjp_targets<<<grid_for(nt), 256, 0, c->stream>>>(nt, kind, c->out16.ptr, dout, r_tpos);
+      FMM_CUDA_TRY(cudaGetLastError());
+    }
+    const cudaMemcpyKind dir = mem == FMM_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    FMM_CUDA_TRY(cudaMemcpyAsync(target->out, c->out16.ptr, 16 * (size_t)nt * sizeof(double), dir, c->stream));
+    FMM_CUDA_TRY(cudaMemcpyAsync(d_strength, r_str, (size_t)sdim * ns * sizeof(double), dir, c->stream));
+    FMM_CUDA_TRY(cudaMemcpyAsync(d_source_position, r_pos, 3 * (size_t)ns * sizeof(double), dir, c->stream));
+    if (!self && d_target_position)
+      FMM_CUDA_TRY(cudaMemcpyAsync(d_target_position, r_tpos, 3 * (size_t)nt * sizeof(double), dir, c->stream));
+    FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return FMM_OK;
   } catch (const Error& e) {
     return fail(c, e);

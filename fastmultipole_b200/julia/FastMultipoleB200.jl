@@ -200,4 +200,48 @@ end
 
 direct!(system; kwargs...) = direct!(system, system; kwargs...)
 
+"""
+    vjp(system, cotangent; targets=nothing, kwargs...)
+
+Gradient of a scalar loss through `fmm!` (the adjoint FMM; the reference obtains it
+by differentiating `fmm!` with ReverseDiff, README.md:19).  `cotangent` is dL/dphi per
+target (point sources) or dL/du (3 x n_t, vortex particles).  Returns
+`(d_strength, d_position, d_target_position)`; the last is `nothing` when the sources
+are the targets.  Keyword arguments as `fmm!`.
+"""
+function vjp(system, cotangent; targets=nothing, expansion_order=5, leaf_size=20, multipole_acceptance=0.4,
+             error_tolerance=nothing, shrink_recenter=true, interaction_list_method=SelfTuningTreeStop(),
+             precision=:f64)
+    buf = source_buffer(system)
+    n_s = size(buf, 2)
+    vortex = has_vector_potential(system)
+    self_eval = targets === nothing
+    n_t = self_eval ? n_s : get_n_bodies(targets)
+    pos = self_eval ? buf : reduce(hcat, [Vector{Float64}(get_position(targets, i)) for i in 1:n_t])
+    d_out = zeros(Float64, 16, n_t)
+    if vortex
+        d_out[5:7, :] .= reshape(cotangent, 3, n_t)
+    else
+        d_out[4, :] .= vec(cotangent)
+    end
+    out = zeros(Float64, 16, n_t)
+    d_str = zeros(Float64, vortex ? 3 : 1, n_s)
+    d_pos = zeros(Float64, 3, n_s)
+    d_tpos = self_eval ? zeros(Float64, 3, 0) : zeros(Float64, 3, n_t)
+    em, eps, be = error_code(error_tolerance)
+    opt = FmmOptions(expansion_order, leaf_size, 0, multipole_acceptance, em, eps, be, shrink_recenter,
+                     list_code(interaction_list_method), 1, 1, 1, 1, 1, 1, 1, 1, 0, precision == :mixed ? 1 : 0)
+    res = FmmResult()
+    GC.@preserve buf pos out d_out d_str d_pos d_tpos begin
+        src = FmmSourceSystem(kernel_kind(system), n_s, size(buf, 1), pointer(buf), 0)
+        tgt = FmmTargetSystem(n_t, self_eval ? Ptr{Cdouble}(C_NULL) : pointer(pos), 3, pointer(out), 0)
+        check(ccall((:fmm_vjp, libfmm), Cint,
+                    (Ptr{Cvoid}, Ref{FmmTargetSystem}, Ref{FmmSourceSystem}, Ref{FmmOptions}, Ptr{Cdouble},
+                     Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ref{FmmResult}),
+                    context(), tgt, src, opt, pointer(d_out), pointer(d_str), pointer(d_pos),
+                    self_eval ? Ptr{Cdouble}(C_NULL) : pointer(d_tpos), res))
+    end
+    return vortex ? d_str : vec(d_str), d_pos, self_eval ? nothing : d_tpos
+end
+
 end # module

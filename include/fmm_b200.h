@@ -158,6 +158,31 @@ FMM_API int fmm_solve(fmm_ctx* ctx, const fmm_target_system* target, const fmm_s
 FMM_API int fmm_direct(fmm_ctx* ctx, const fmm_target_system* target, const fmm_source_system* source,
                int scalar_potential, int gradient, int hessian, int precision);
 
+/* ---- adjoint (vector-Jacobian product) ----------------------------------------
+ * Gradients of a scalar loss L through fmm!: given the cotangents d_out = dL/d(target
+ * buffer) (16 x n_t, body-major, the layout of target->out), returns dL/dstrength,
+ * dL/d(source position) and, for a separate target system, dL/d(target position).
+ * The reference provides this through automatic differentiation of fmm! (README.md:19;
+ * no reference test pins it).  Here it is two solves with the same options: the
+ * forward solve (written to target->out, as fmm_solve) and the adjoint solve, whose
+ * sources sit at the targets with the cotangents as strengths and whose targets are
+ * the sources:
+ *   point sources (kind 1): reads row 4 (phi) of d_out, w_t = dL/dphi_t;
+ *     dL/dq_s = psi(x_s), dL/dx_s = -q_s g_psi(x_s) [- w_s g(x_s) when the sources are
+ *     the targets], dL/dy_t = -w_t g(y_t), with psi, g_psi the adjoint solve's potential
+ *     and gradient rows and g the forward gradient rows;
+ *   vortex particles (kind 3): reads rows 5..7 (u) of d_out, w_t = dL/du_t;
+ *     dL/dGamma_s = u_w(x_s), (dL/dx_s)_i = sum_c Gamma_sc du_w,c/dx_i [+ sum_c w_sc
+ *     du_c/dx_i when the sources are the targets], (dL/dy_t)_i = sum_c w_tc du_c/dx_i(y_t).
+ * Cotangents on the gradient rows of point sources would need dipole sources and are
+ * not read.  The result is the exact gradient of the continuous problem evaluated to
+ * the FMM's accuracy.  All arrays use source->memory; d_strength holds 1 (kind 1) or 3
+ * (kind 3) values per source, the position gradients 3 per body; d_target_position
+ * may be NULL and is not written when target->positions == NULL. */
+FMM_API int fmm_vjp(fmm_ctx* ctx, const fmm_target_system* target, const fmm_source_system* source,
+                    const fmm_options* options, const double* d_out, double* d_strength, double* d_source_position,
+                    double* d_target_position, fmm_result* result);
+
 /* ---- direct! without device allocations --------------------------------------
  * No counterpart in the reference: an all-pairs direct! (same kernels as
  * fmm_direct) for callers that cannot allocate device memory -- code running
