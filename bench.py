@@ -69,6 +69,14 @@ def gen_ring(n, seed):
     return b
 
 
+def gen_c4(n, seed):
+    rng = np.random.default_rng(seed)
+    b = np.zeros((n, 5))
+    b[:, :3] = rng.random((n, 3))
+    b[:, 4] = rng.random(n)
+    return b
+
+
 METRIC = "FMM bodies/sec at <=1e-6 rel err vs FP64 direct, mixed vs FP64"
 
 WORKLOADS = {
@@ -79,6 +87,10 @@ WORKLOADS = {
     "c1": dict(workload="uniform point sources N=1e4, p=6, leaf 50, MAC 0.5", n=10_000, gen=gen_uniform, seed=1,
                kind=1, p=6, ls=50, mac=0.5, err=None, ps=True, gs=True, hs=False, flops_per_pair=20,
                n_cpu=10_000),
+    "c4": dict(workload="adjoint: 200k sources U[0,1]^3, 10k probes U[-0.5,1.5]^3, p=8, loss sum(phi^2), "
+                        "gradients wrt strengths and positions", n=200_000, n_probes=10_000, gen=gen_c4, seed=4,
+               kind=1, p=8, ls=50, mac=0.5, err=None, ps=True, gs=True, hs=False, flops_per_pair=20,
+               n_cpu=20_000),
     "c3": dict(workload="vortex ring N=2e6 (R=1, core sigma 0.05), p=12, leaf 80, MAC 0.4, velocity + gradient",
                n=2_000_000, gen=gen_ring, seed=3, kind=3, p=12, ls=80, mac=0.4, err=None, ps=False, gs=True,
                hs=True, flops_per_pair=72, n_cpu=40_000),
@@ -343,6 +355,100 @@ def gpu_arm(args, w, rank, world, local_rank):
     ctx.close()
 
 
+def vjp_arm(args, w):
+    """Adjoint workload: one step = forward solve at the probes (phi), then fmm_vjp with
+    dL/dphi = 2 phi (L = sum phi^2); device-resident inputs; CUDA-event timing."""
+    import torch
+    import fastmultipole_b200 as fm
+    from fastmultipole_b200 import _lib as L
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    ctx = fm.Context(0)
+    ctx.set_stream(stream.cuda_stream)
+    lib = L.lib()
+    n, npr = w["n"], w["n_probes"]
+    buf = w["gen"](n, w["seed"])
+    probes = -0.5 + 2.0 * np.random.default_rng(w["seed"] + 1).random((npr, 3))
+    src_dev = torch.from_numpy(buf).to(dev)
+    pr_dev = torch.from_numpy(probes).to(dev)
+    out_dev = torch.empty((npr, 16), dtype=torch.float64, device=dev)
+    dout = torch.zeros((npr, 16), dtype=torch.float64, device=dev)
+    dq = torch.empty(n, dtype=torch.float64, device=dev)
+    dx = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    dy = torch.empty((npr, 3), dtype=torch.float64, device=dev)
+    src = L.SourceSystem(1, n, 5, src_dev.data_ptr(), L.FMM_MEMORY_DEVICE)
+    tgt = L.TargetSystem(npr, pr_dev.data_ptr(), 3, out_dev.data_ptr(), L.FMM_MEMORY_DEVICE)
+    opt = fm.make_options(expansion_order=w["p"], leaf_size_source=w["ls"], multipole_acceptance=w["mac"],
+                          scalar_potential=True, gradient=True)
+    res = L.Result()
+    dp = L._dp
+
+    def step():
+        ctx.check(lib.fmm_solve(ctx.handle, C.byref(tgt), C.byref(src), C.byref(opt), C.byref(res)))
+        dout[:, 3] = 2.0 * out_dev[:, 3]
+        ctx.check(lib.fmm_vjp(ctx.handle, C.byref(tgt), C.byref(src), C.byref(opt),
+                              C.cast(dout.data_ptr(), dp), C.cast(dq.data_ptr(), dp), C.cast(dx.data_ptr(), dp),
+                              C.cast(dy.data_ptr(), dp), C.byref(res)))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    # central finite differences of the exact loss (all-pairs direct) on 16 coordinates
+    phi = np.zeros((npr, 16))
+
+    def loss(b, pr):
+        bb = np.ascontiguousarray(b)
+        pp = np.ascontiguousarray(pr)
+        s_ = L.SourceSystem(1, n, 5, bb.ctypes.data, L.FMM_MEMORY_HOST)
+        t_ = L.TargetSystem(npr, pp.ctypes.data, 3, phi.ctypes.data, L.FMM_MEMORY_HOST)
+        ctx.check(lib.fmm_direct(ctx.handle, C.byref(t_), C.byref(s_), 1, 0, 0, L.FMM_PRECISION_F64))
+        return float(np.sum(phi[:, 3] ** 2))
+
+    gq, gx, gy = dq.cpu().numpy(), dx.cpu().numpy(), dy.cpu().numpy()
+    rng = np.random.default_rng(9)
+    errs = []
+    h = 1e-6
+    for _ in range(16):
+        which = rng.integers(0, 3)
+        if which == 0:
+            i = rng.integers(0, n)
+            bp, bm = buf.copy(), buf.copy()
+            hq = 1e-3 * buf[i, 4]
+            bp[i, 4] += hq
+            bm[i, 4] -= hq
+            fd = (loss(bp, probes) - loss(bm, probes)) / (2 * hq)
+            errs.append(abs(gq[i] - fd) / np.abs(gq).max())
+        elif which == 1:
+            i, k = rng.integers(0, n), rng.integers(0, 3)
+            bp, bm = buf.copy(), buf.copy()
+            bp[i, k] += h
+            bm[i, k] -= h
+            fd = (loss(bp, probes) - loss(bm, probes)) / (2 * h)
+            errs.append(abs(gx[i, k] - fd) / np.abs(gx).max())
+        else:
+            i, k = rng.integers(0, npr), rng.integers(0, 3)
+            pp, pm = probes.copy(), probes.copy()
+            pp[i, k] += h
+            pm[i, k] -= h
+            fd = (loss(buf, pp) - loss(buf, pm)) / (2 * h)
+            errs.append(abs(gy[i, k] - fd) / np.abs(gy).max())
+    line = {"metric": "FMM loss gradient (forward + adjoint) sources/s", "value": n / (ms * 1e-3),
+            "unit": "sources/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": w["workload"], "n_sources": n, "n_probes": npr, "solves_per_step": 3},
+            "fd_max_rel_dev": float(max(errs)), "fd_coordinates": 16}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -359,6 +465,15 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.config == "c4":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference differentiates fmm! with "
+                                  "ReverseDiff (Julia), absent on this image; the CPU port has no adjoint"}))
+            return
+        if rank == 0:
+            vjp_arm(args, w)
+        return
     if args.impl == "reference":
         reference_arm(args, w, rank)
         return
