@@ -91,6 +91,10 @@ WORKLOADS = {
                         "gradients wrt strengths and positions", n=200_000, n_probes=10_000, gen=gen_c4, seed=4,
                kind=1, p=8, ls=50, mac=0.5, err=None, ps=True, gs=True, hs=False, flops_per_pair=20,
                n_cpu=20_000),
+    "c5": dict(workload="serving: requests with N log-uniform [1e3, 5e5], half point sources / half vortex, uniform "
+                        "cube or 8 Gaussians, PowerRelativeGradient tolerance log-uniform [1e-8, 1e-4] (p <= 16), "
+                        "Poisson arrivals at ~70% of the measured capacity", n_requests=256, seed=5, workers=4,
+               kind=1, n=0, n_cpu=0),
     "c3": dict(workload="vortex ring N=2e6 (R=1, core sigma 0.05), p=12, leaf 80, MAC 0.4, velocity + gradient",
                n=2_000_000, gen=gen_ring, seed=3, kind=3, p=12, ls=80, mac=0.4, err=None, ps=False, gs=True,
                hs=True, flops_per_pair=72, n_cpu=40_000),
@@ -449,6 +453,99 @@ def vjp_arm(args, w):
     ctx.close()
 
 
+def serve_requests(w):
+    """The request mix of the serving workload (seeded)."""
+    rng = np.random.default_rng(w["seed"])
+    reqs = []
+    for k in range(w["n_requests"]):
+        n = int(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
+        kind = 1 if k % 2 == 0 else 3
+        tol = float(np.exp(rng.uniform(np.log(1e-8), np.log(1e-4))))
+        if rng.random() < 0.5:
+            b = gen_uniform(n, int(rng.integers(1 << 30)))
+        else:
+            b = gen_clustered(n, int(rng.integers(1 << 30)))
+        if kind == 3:
+            v = np.zeros((n, 7))
+            v[:, :4] = b[:, :4]
+            v[:, 4:7] = (2 * rng.random((n, 3)) - 1) / n
+            b = v
+        reqs.append((b, kind, tol))
+    return reqs
+
+
+def serve_arm(args, w):
+    """Serving workload: the request mix is run back to back to measure the capacity,
+    then replayed with Poisson arrivals at 70% of it; latency = completion - arrival."""
+    import threading
+    import fastmultipole_b200 as fm
+    from fastmultipole_b200 import _lib as L
+    reqs = serve_requests(w)
+    ctx = fm.Context(0)
+    server = fm.Server(n_workers=w["workers"], hbm_budget=150 << 30, ctx=ctx)
+
+    def opt_of(kind, tol):
+        return fm.make_options(expansion_order=16, leaf_size_source=64 if kind == 1 else 80,
+                               multipole_acceptance=0.5, error_tolerance=fm.PowerRelativeGradient(tol),
+                               scalar_potential=kind == 1, precision="f64")
+
+    # warm-up (tables, allocations on every worker)
+    for b, kind, tol in reqs[: 2 * w["workers"]]:
+        server.poll(server.submit(b, kind, opt_of(kind, tol)))
+    # capacity: all requests queued at once
+    t0 = time.perf_counter()
+    ids = [server.submit(b, kind, opt_of(kind, tol)) for b, kind, tol in reqs]
+    for rid in ids:
+        rc, _, _ = server.poll(rid)
+        assert rc == L.FMM_OK
+    cap = len(reqs) / (time.perf_counter() - t0)
+    rate = 0.7 * cap
+    gaps = np.random.default_rng(w["seed"] + 1).exponential(1.0 / rate, len(reqs))
+    arrive = np.cumsum(gaps)
+    done_at = {}
+    outstanding = {}
+    lock = threading.Lock()
+    finished = threading.Event()
+
+    def poller():
+        while not (finished.is_set() and not outstanding):
+            with lock:
+                items = list(outstanding.items())
+            for rid, k in items:
+                rc, _, _ = server.poll(rid, 0)
+                if rc != L.FMM_PENDING:
+                    done_at[k] = time.perf_counter()
+                    with lock:
+                        outstanding.pop(rid, None)
+            time.sleep(1e-4)
+
+    th = threading.Thread(target=poller)
+    th.start()
+    t0 = time.perf_counter()
+    for k, (b, kind, tol) in enumerate(reqs):
+        delay = t0 + arrive[k] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        rid = server.submit(b, kind, opt_of(kind, tol))
+        with lock:
+            outstanding[rid] = k
+    finished.set()
+    th.join()
+    lat = np.array([1e3 * (done_at[k] - (t0 + arrive[k])) for k in range(len(reqs))])
+    server.stop()
+    ctx.close()
+    ns = np.array([len(r[0]) for r in reqs])
+    line = {"metric": "serve latency p50 ms", "value": float(np.percentile(lat, 50)), "unit": "ms",
+            "p99_ms": float(np.percentile(lat, 99)), "p90_ms": float(np.percentile(lat, 90)),
+            "capacity_requests_per_s": cap, "offered_requests_per_s": rate,
+            "capacity_bodies_per_s": float(ns.sum() * cap / len(reqs)), "n_gpus": 1,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": w["workload"], "requests": len(reqs), "workers": w["workers"],
+                       "bodies_total": int(ns.sum()), "hbm_budget_gb": 150}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -465,6 +562,15 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.config == "c5":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference runs one fmm! at a time "
+                                  "(Julia, absent on this image); no serving loop to time"}))
+            return
+        if rank == 0:
+            serve_arm(args, w)
+        return
     if args.config == "c4":
         if args.impl == "reference":
             if rank == 0:

@@ -9,7 +9,8 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfmmb200.so")
 
-FMM_OK, FMM_ERR_ARGUMENT, FMM_ERR_CUDA, FMM_ERR_NO_DEVICE, FMM_ERR_TREE_DEPTH, FMM_ERR_MEMORY, FMM_ERR_STATE = range(7)
+(FMM_OK, FMM_ERR_ARGUMENT, FMM_ERR_CUDA, FMM_ERR_NO_DEVICE, FMM_ERR_TREE_DEPTH, FMM_ERR_MEMORY, FMM_ERR_STATE,
+ FMM_PENDING) = range(8)
 FMM_POINT_SOURCE, FMM_POINT_VORTEX = 1, 3
 FMM_LIST_SELF_TUNING_TREE_STOP, FMM_LIST_BARBA, FMM_LIST_SELF_TUNING = 0, 1, 2
 FMM_ERROR_NONE = 0
@@ -21,7 +22,7 @@ FMM_PRECISION_F64, FMM_PRECISION_MIXED = 0, 1
 FMM_MEMORY_HOST, FMM_MEMORY_DEVICE = 0, 1
 
 STATUS_NAMES = {0: "FMM_OK", 1: "FMM_ERR_ARGUMENT", 2: "FMM_ERR_CUDA", 3: "FMM_ERR_NO_DEVICE",
-                4: "FMM_ERR_TREE_DEPTH", 5: "FMM_ERR_MEMORY", 6: "FMM_ERR_STATE"}
+                4: "FMM_ERR_TREE_DEPTH", 5: "FMM_ERR_MEMORY", 6: "FMM_ERR_STATE", 7: "FMM_PENDING"}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -70,6 +71,10 @@ class TreeView(C.Structure):
                [(n, _i64p) for n in ("sort_index", "levels_start", "levels_end", "leaf_index")]
 
 
+class Request(C.Structure):
+    _fields_ = [("target", TargetSystem), ("source", SourceSystem), ("options", Options)]
+
+
 # every entry point of include/fmm_b200.h with its ctypes signature
 SIGNATURES = {
     "fmm_ctx_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int]),
@@ -86,6 +91,10 @@ SIGNATURES = {
                              C.c_int, C.c_int]),
     "fmm_vjp": (C.c_int, [C.c_void_p, C.POINTER(TargetSystem), C.POINTER(SourceSystem), C.POINTER(Options), _dp, _dp,
                           _dp, _dp, C.POINTER(Result)]),
+    "fmm_serve_start": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t]),
+    "fmm_serve_submit": (C.c_int, [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)]),
+    "fmm_serve_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Result), C.c_int]),
+    "fmm_serve_stop": (C.c_int, [C.c_void_p]),
     "fmm_direct_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.POINTER(TargetSystem), C.POINTER(SourceSystem), C.c_int,
                                      C.c_int, C.c_int, C.c_int]),
     "fmm_get_tree": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TreeView)]),

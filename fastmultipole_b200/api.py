@@ -425,6 +425,47 @@ def vjp(system, d_potential=None, d_velocity=None, targets=None, *, leaf_size=20
     return r
 
 
+class Server:
+    """Concurrent fmm! requests on one device (fmm_serve_*): ``n_workers`` solver
+    contexts run queued requests as soon as one finishes; each worker's HBM budget
+    is ``hbm_budget / n_workers`` (0: unlimited)."""
+
+    def __init__(self, n_workers=4, hbm_budget=0, ctx=None):
+        self.ctx = ctx or default_context()
+        self.ctx.check(L.lib().fmm_serve_start(self.ctx.handle, int(n_workers), int(hbm_budget)))
+        self._live = {}
+
+    def submit(self, source_buf, kind, opt, target_pos=None):
+        """Queue one fmm! on raw buffers; returns the request id."""
+        sb = np.ascontiguousarray(source_buf, dtype=np.float64)
+        n_s, d = sb.shape
+        if target_pos is None:
+            tp = None
+            out = np.zeros((n_s, 16))
+            tgt = L.TargetSystem(n_s, None, 0, out.ctypes.data, L.FMM_MEMORY_HOST)
+        else:
+            tp = np.ascontiguousarray(target_pos, dtype=np.float64)
+            out = np.zeros((len(tp), 16))
+            tgt = L.TargetSystem(len(tp), tp.ctypes.data, 3, out.ctypes.data, L.FMM_MEMORY_HOST)
+        req = L.Request(tgt, L.SourceSystem(kind, n_s, d, sb.ctypes.data, L.FMM_MEMORY_HOST), opt)
+        rid = C.c_uint64(0)
+        self.ctx.check(L.lib().fmm_serve_submit(self.ctx.handle, C.byref(req), C.byref(rid)))
+        self._live[rid.value] = (sb, tp, out, req)  # the buffers stay alive until the request is polled
+        return rid.value
+
+    def poll(self, rid, timeout_ms=-1):
+        """Returns (status, out, fmm_result); status FMM_PENDING if not finished."""
+        res = L.Result()
+        rc = L.lib().fmm_serve_poll(self.ctx.handle, C.c_uint64(rid), C.byref(res), int(timeout_ms))
+        if rc == L.FMM_PENDING:
+            return rc, None, None
+        _, _, out, _ = self._live.pop(rid)
+        return rc, out, res
+
+    def stop(self):
+        self.ctx.check(L.lib().fmm_serve_stop(self.ctx.handle))
+
+
 def fmm(target_systems, source_systems=None, *, leaf_size=None, leaf_size_source=None, leaf_size_target=None,
         expansion_order=5, multipole_acceptance=0.4, error_tolerance=None, shrink_recenter=True,
         interaction_list_method=None, scalar_potential=False, gradient=True, hessian=False, farfield=True,

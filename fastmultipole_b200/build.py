@@ -17,7 +17,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 # the octree and the interaction lists must reproduce the reference's FP64
 # comparisons bit for bit: no fused multiply-adds there
 EXACT = {"tree.cu", "lists.cu"}
-SOURCES = ["tables.cpp", "tree.cu", "lists.cu", "p2p.cu", "expansions.cu", "m2l_lane.cu", "api.cu", "noalloc.cu"]
+SOURCES = ["tables.cpp", "tree.cu", "lists.cu", "p2p.cu", "expansions.cu", "m2l_lane.cu", "api.cu", "noalloc.cu",
+           "serve.cpp"]
 
 
 def _nvcc():

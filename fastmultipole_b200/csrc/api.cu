@@ -127,7 +127,13 @@ struct fmm_ctx {
   bool have_solve = false;
   int last_p = 0;
   int last_kind = 1;
+  void* serve = nullptr;  // serving state (serve.cpp)
 };
+
+namespace fmmb {
+void*& ctx_serve_slot(fmm_ctx* c) { return c->serve; }
+int ctx_device(fmm_ctx* c) { return c->device; }
+}  // namespace fmmb
 
 namespace {
 
@@ -394,6 +400,7 @@ int fmm_ctx_create(fmm_ctx** out, int device) {
 
 int fmm_ctx_destroy(fmm_ctx* c) {
   if (!c) return FMM_OK;
+  if (c->serve) fmm_serve_stop(c);
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   for (Workspace* w : {&c->main, &c->est}) {

@@ -45,7 +45,8 @@ typedef enum {
   FMM_ERR_NO_DEVICE = 3,   /* no usable sm_100 device                               */
   FMM_ERR_TREE_DEPTH = 4,  /* bodies too clustered for the 21-level octant key     */
   FMM_ERR_MEMORY = 5,      /* the request exceeds the context's HBM budget          */
-  FMM_ERR_STATE = 6        /* export requested before any solve                     */
+  FMM_ERR_STATE = 6,       /* export requested before any solve / server not running */
+  FMM_PENDING = 7          /* fmm_serve_poll: the request has not finished yet       */
 } fmm_status;
 
 /* body_to_multipole!(system, ...) = body_to_multipole!(Point{Source|Vortex}, ...)
@@ -182,6 +183,31 @@ FMM_API int fmm_direct(fmm_ctx* ctx, const fmm_target_system* target, const fmm_
 FMM_API int fmm_vjp(fmm_ctx* ctx, const fmm_target_system* target, const fmm_source_system* source,
                     const fmm_options* options, const double* d_out, double* d_strength, double* d_source_position,
                     double* d_target_position, fmm_result* result);
+
+/* ---- serving: concurrent requests on one device -------------------------------
+ * The reference reuses a Cache across fmm! calls (src/containers.jl:264-292) and runs
+ * one call at a time.  A serving context keeps n_workers solver contexts, each with
+ * its own stream and resident buffers, and runs queued requests concurrently: a
+ * worker takes the next request as soon as it finishes one.  Each worker's HBM
+ * budget is hbm_budget_bytes / n_workers (0 = unlimited); a request that does not fit
+ * finishes with FMM_ERR_MEMORY.  A request's result does not depend on what else is
+ * running (each request runs the deterministic fmm_solve path on its own buffers).
+ * The caller keeps every buffer of a request alive until fmm_serve_poll has
+ * returned something other than FMM_PENDING for its id; each id is polled to
+ * completion once.  fmm_ctx_destroy stops the server. */
+typedef struct {
+  fmm_target_system target; /* target.out receives the 16-row buffer, as in fmm_solve */
+  fmm_source_system source;
+  fmm_options options;
+} fmm_request;
+
+FMM_API int fmm_serve_start(fmm_ctx* ctx, int n_workers, size_t hbm_budget_bytes);
+FMM_API int fmm_serve_submit(fmm_ctx* ctx, const fmm_request* request, uint64_t* id);
+/* waits up to timeout_ms (< 0: without limit); returns the request's fmm_solve status,
+ * or FMM_PENDING if it has not finished (the request stays queued) */
+FMM_API int fmm_serve_poll(fmm_ctx* ctx, uint64_t id, fmm_result* result, int timeout_ms);
+/* finishes the queued requests, then stops the workers */
+FMM_API int fmm_serve_stop(fmm_ctx* ctx);
 
 /* ---- direct! without device allocations --------------------------------------
  * No counterpart in the reference: an all-pairs direct! (same kernels as

@@ -44,7 +44,7 @@ def test_struct_layouts_match_the_header(tmp_path):
     """Compile a probe against include/fmm_b200.h and compare sizes/offsets with the ctypes mirrors."""
     import subprocess
     structs = {"fmm_options": L.Options, "fmm_source_system": L.SourceSystem, "fmm_target_system": L.TargetSystem,
-               "fmm_result": L.Result, "fmm_tree_view": L.TreeView}
+               "fmm_result": L.Result, "fmm_tree_view": L.TreeView, "fmm_request": L.Request}
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "fmm_b200.h"', "int main(void){"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
