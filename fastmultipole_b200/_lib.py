@@ -89,6 +89,8 @@ SIGNATURES = {
                             C.POINTER(Result)]),
     "fmm_direct": (C.c_int, [C.c_void_p, C.POINTER(TargetSystem), C.POINTER(SourceSystem), C.c_int, C.c_int,
                              C.c_int, C.c_int]),
+    "fmm_solve_multi": (C.c_int, [C.c_void_p, C.POINTER(TargetSystem), C.POINTER(SourceSystem), C.c_int,
+                                  C.POINTER(Options), C.POINTER(Result)]),
     "fmm_vjp": (C.c_int, [C.c_void_p, C.POINTER(TargetSystem), C.POINTER(SourceSystem), C.POINTER(Options), _dp, _dp,
                           _dp, _dp, C.POINTER(Result)]),
     "fmm_serve_start": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t]),

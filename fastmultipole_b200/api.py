@@ -362,6 +362,22 @@ def solve_buffers(source_buf, kind, opt, target_pos=None, ctx=None, timing=False
     return out, res
 
 
+def solve_multi_buffers(sources, opt, target_pos, ctx=None):
+    """fmm! of several source systems on raw buffers: ``sources`` is a list of
+    (buffer (N_k, d_k), kind); the target buffers of the per-system solves are summed
+    (fmm_solve_multi).  Returns (out (Nt, 16), fmm_result)."""
+    ctx = ctx or default_context()
+    bufs = [np.ascontiguousarray(b, dtype=np.float64) for b, _ in sources]
+    arr = (L.SourceSystem * len(bufs))(*[L.SourceSystem(k, b.shape[0], b.shape[1], b.ctypes.data, L.FMM_MEMORY_HOST)
+                                         for b, (_, k) in zip(bufs, sources)])
+    tp = np.ascontiguousarray(target_pos, dtype=np.float64)
+    out = np.zeros((len(tp), 16))
+    tgt = L.TargetSystem(len(tp), tp.ctypes.data, 3, out.ctypes.data, L.FMM_MEMORY_HOST)
+    res = L.Result()
+    ctx.check(L.lib().fmm_solve_multi(ctx.handle, C.byref(tgt), arr, len(bufs), C.byref(opt), C.byref(res)))
+    return out, res
+
+
 def vjp_buffers(source_buf, kind, opt, d_out, target_pos=None, ctx=None):
     """Gradients of a loss through fmm! on raw buffers (fmm_vjp).
 
@@ -484,11 +500,23 @@ def fmm(target_systems, source_systems=None, *, leaf_size=None, leaf_size_source
     targets = _tuple(target_systems)
     sources = targets if self_eval else _tuple(source_systems)
     ls_s = leaf_size_source or leaf_size or 20
-    kind = _kind(sources)
     opt = make_options(expansion_order, ls_s, leaf_size_target or (leaf_size if self_eval else None),
                        multipole_acceptance, error_tolerance, shrink_recenter, interaction_list_method, farfield,
                        nearfield, self_induced, upward_pass, horizontal_pass, downward_pass, scalar_potential,
                        gradient, hessian, precision)
+    if len({s.kernel for s in sources}) > 1:
+        # systems of different kernels: one solve per kernel on the same targets, summed
+        groups = {}
+        for s in sources:
+            groups.setdefault(_kind((s,)), []).append(s)
+        out, res = solve_multi_buffers([(_source_buffer(g, k), k) for k, g in groups.items()], opt,
+                                       _positions(targets), ctx)
+        switch = DerivativesSwitch(bool(scalar_potential), bool(gradient), bool(hessian))
+        _scatter(targets, out, switch)
+        optimized = dict(leaf_size_source=ls_s, expansion_order=max(expansion_order, 1),
+                         multipole_acceptance=multipole_acceptance)
+        return (optimized, ctx, None, None, None, None, tuple(switch for _ in targets), bool(res.error_success))
+    kind = _kind(sources)
     buf = _source_buffer(sources, kind)
     same = self_eval or all(a is b for a, b in zip(targets, sources)) and len(targets) == len(sources)
     tpos = None if same else _positions(targets)

@@ -42,6 +42,14 @@ __global__ void k_unsort(const double* __restrict__ acc13, const int* __restrict
 
 int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); }
 
+// out += in on rows 4..16 of the target buffer (rows 1..3 are the positions)
+__global__ void k_add_rows(int64_t n, const double* __restrict__ in, double* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 13 * n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = i / 13, r = 3 + i % 13;
+    out[16 * b + r] += in[16 * b + r];
+  }
+}
+
 // adjoint sources: at the targets (or the sources themselves), strengths = cotangents
 __global__ void k_adj_sources(int64_t n, const double* __restrict__ pos, int64_t stride, bool radius_from_pos,
                               const double* __restrict__ dout16, int kind, double* __restrict__ buf) {
@@ -123,6 +131,7 @@ struct fmm_ctx {
   DevTables tables;
   DevBuf<double> stage_s, stage_t, out16, est_out16;
   DevBuf<double> adj_src, adj_out16, stage_d, vjp_out;  // fmm_vjp
+  DevBuf<double> multi16;                                // fmm_solve_multi
   DevBuf<int> stats;
   bool have_solve = false;
   int last_p = 0;
@@ -423,6 +432,7 @@ int fmm_ctx_destroy(fmm_ctx* c) {
   c->adj_out16.release();
   c->stage_d.release();
   c->vjp_out.release();
+  c->multi16.release();
   c->stats.release();
   delete c;
   return FMM_OK;
@@ -457,7 +467,7 @@ size_t fmm_ctx_device_bytes(const fmm_ctx* c) {
        (s.vals_a.cap + s.vals_b.cap + s.tmp_i.cap + s.tmp_j.cap + s.tmp_k.cap + s.cnt_a.cap + s.cnt_b.cap) * 4 +
        (s.front_a.cap + s.front_b.cap + s.dir_raw.cap + s.m2l_raw.cap) * 8 + s.tmp_d.cap * 8;
   b += (c->stage_s.cap + c->stage_t.cap + c->out16.cap + c->est_out16.cap) * 8;
-  b += (c->adj_src.cap + c->adj_out16.cap + c->stage_d.cap + c->vjp_out.cap) * 8;
+  b += (c->adj_src.cap + c->adj_out16.cap + c->stage_d.cap + c->vjp_out.cap + c->multi16.cap) * 8;
   return b;
 }
 
@@ -519,6 +529,82 @@ int fmm_solve(fmm_ctx* c, const fmm_target_system* target, const fmm_source_syst
     c->have_solve = true;
     c->last_p = opt->expansion_order;
     c->last_kind = source->kind;
+    return FMM_OK;
+  } catch (const Error& e) {
+    return fail(c, e);
+  }
+}
+
+int fmm_solve_multi(fmm_ctx* c, const fmm_target_system* target, const fmm_source_system* sources, int n_sources,
+                    const fmm_options* opt, fmm_result* result) {
+  if (!c) return FMM_ERR_ARGUMENT;
+  if (n_sources == 1 && sources) return fmm_solve(c, target, sources, opt, result);
+  try {
+    FMM_CHECK(sources && n_sources > 1, FMM_ERR_ARGUMENT, "fmm_solve_multi: no source systems");
+    FMM_CHECK(target && target->positions, FMM_ERR_ARGUMENT,
+              "fmm_solve_multi: several source systems need explicit target positions");
+    FMM_CHECK(target->stride >= 3, FMM_ERR_ARGUMENT, "target stride must be >= 3");
+    FMM_CHECK(opt != nullptr, FMM_ERR_ARGUMENT, "options are NULL");
+    const int64_t nt = target->n_bodies;
+    FMM_CHECK(nt == 0 || target->out, FMM_ERR_ARGUMENT, "target out buffer is NULL");
+    FMM_CUDA_TRY(cudaSetDevice(c->device));
+    fmm_result total;
+    std::memset(&total, 0, sizeof(total));
+    total.error_success = 1;
+    // every solve sees device-resident targets: the positions (staged once) and an output buffer
+    fmm_target_system td = *target;
+    td.memory = FMM_MEMORY_DEVICE;
+    if (nt > 0) {
+      c->multi16.grow(16 * (size_t)nt);
+      c->vjp_out.grow(16 * (size_t)nt);
+      if (target->memory == FMM_MEMORY_HOST) {
+        c->stage_d.grow(3 * (size_t)nt);
+        FMM_CUDA_TRY(cudaMemcpy2DAsync(c->stage_d.ptr, 3 * sizeof(double), target->positions,
+                                       target->stride * sizeof(double), 3 * sizeof(double), nt,
+                                       cudaMemcpyHostToDevice, c->stream));
+        td.positions = c->stage_d.ptr;
+        td.stride = 3;
+      }
+    }
+    for (int k = 0; k < n_sources; ++k) {
+      td.out = k == 0 ? c->multi16.ptr : c->vjp_out.ptr;
+      fmm_result r;
+      std::memset(&r, 0, sizeof(r));
+      const int rc = fmm_solve(c, &td, &sources[k], opt, &r);
+      if (rc != FMM_OK) return rc;
+      if (nt > 0 && k > 0) {
+        note_launch();
+        k_add_rows<<<grid_for(13 * nt), 256, 0, c->stream>>>(nt, c->vjp_out.ptr, c->multi16.ptr);
+        FMM_CUDA_TRY(cudaGetLastError());
+      }
+      total.p_max = std::max(total.p_max, r.p_max);
+      total.error_success = total.error_success && r.error_success;
+      total.n_target_branches += r.n_target_branches;
+      total.n_source_branches += r.n_source_branches;
+      total.n_target_leaves += r.n_target_leaves;
+      total.n_source_leaves += r.n_source_leaves;
+      total.n_m2l += r.n_m2l;
+      total.n_direct += r.n_direct;
+      total.n_p2p_pairs += r.n_p2p_pairs;
+      total.m2l_flops += r.m2l_flops;
+      total.t_total_ms += r.t_total_ms;
+      total.t_tree_ms += r.t_tree_ms;
+      total.t_lists_ms += r.t_lists_ms;
+      total.t_influence_ms += r.t_influence_ms;
+      total.t_nearfield_ms += r.t_nearfield_ms;
+      total.t_upward_ms += r.t_upward_ms;
+      total.t_horizontal_ms += r.t_horizontal_ms;
+      total.t_downward_ms += r.t_downward_ms;
+      total.n_kernel_launches += r.n_kernel_launches;
+    }
+    if (nt > 0) {
+      const cudaMemcpyKind dir =
+          target->memory == FMM_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+      FMM_CUDA_TRY(cudaMemcpyAsync(target->out, c->multi16.ptr, 16 * (size_t)nt * sizeof(double), dir, c->stream));
+      FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    }
+    c->have_solve = false;  // the exported trees would be those of the last system only
+    if (result) *result = total;
     return FMM_OK;
   } catch (const Error& e) {
     return fail(c, e);

@@ -159,6 +159,18 @@ FMM_API int fmm_solve(fmm_ctx* ctx, const fmm_target_system* target, const fmm_s
 FMM_API int fmm_direct(fmm_ctx* ctx, const fmm_target_system* target, const fmm_source_system* source,
                int scalar_potential, int gradient, int hessian, int precision);
 
+/* ---- several source systems -----------------------------------------------------
+ * fmm!(targets, (system_1, system_2, ...)) with systems of different kernels (point
+ * sources and vortex particles, src/fmm.jl:807-884 with tuples of systems).  The field
+ * is linear in the sources, so the solve runs once per source system on the same
+ * targets and the target buffers are summed (rows 4..16).  The reference instead
+ * builds one octree over the bodies of all systems; the two agree to the FMM's
+ * accuracy, not to the last digit.  target->positions must be given when
+ * n_sources > 1; n_sources == 1 is fmm_solve.  The result reports the largest order
+ * used, success only if every solve met its tolerance, and summed counts and times. */
+FMM_API int fmm_solve_multi(fmm_ctx* ctx, const fmm_target_system* target, const fmm_source_system* sources,
+                            int n_sources, const fmm_options* options, fmm_result* result);
+
 /* ---- adjoint (vector-Jacobian product) ----------------------------------------
  * Gradients of a scalar loss L through fmm!: given the cotangents d_out = dL/d(target
  * buffer) (16 x n_t, body-major, the layout of target->out), returns dL/dstrength,
