@@ -132,12 +132,38 @@ struct fmm_ctx {
   DevBuf<double> stage_s, stage_t, out16, est_out16;
   DevBuf<double> adj_src, adj_out16, stage_d, vjp_out;  // fmm_vjp
   DevBuf<double> multi16;                                // fmm_solve_multi
+  // influence estimate on its own stream (run_fmm)
+  cudaStream_t est_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  Scratch est_sc;
+  DevBuf<int> est_stats;
   DevBuf<int> stats;
   bool have_solve = false;
   int last_p = 0;
   int last_kind = 1;
   void* serve = nullptr;  // serving state (serve.cpp)
 };
+
+namespace {
+cudaStream_t est_stream(fmm_ctx* c) {
+  if (!c->est_stream) {
+    int least = 0, greatest = 0;
+    FMM_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    FMM_CUDA_TRY(cudaStreamCreateWithPriority(&c->est_stream, cudaStreamNonBlocking, greatest));
+  }
+  return c->est_stream;
+}
+cudaEvent_t fork_event(fmm_ctx* c) {
+  if (!c->ev_fork) FMM_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+  return c->ev_fork;
+}
+cudaEvent_t join_event(fmm_ctx* c) {
+  if (!c->ev_join) FMM_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+  return c->ev_join;
+}
+Scratch& est_scratch(fmm_ctx* c) { return c->est_sc; }
+DevBuf<int>& est_stats(fmm_ctx* c) { return c->est_stats; }
+}  // namespace
 
 namespace fmmb {
 void*& ctx_serve_slot(fmm_ctx* c) { return c->serve; }
@@ -172,20 +198,32 @@ size_t footprint(const SolveIn& in, const fmm_options& o) {
   return exp + bodies + lists + scratch;
 }
 
-// one fmm! evaluation into out16 (device, original target order)
+// stream of the influence estimate: non-blocking, highest priority, so that its small
+// kernels take SM slots as soon as the solve's near-field CTAs retire
+cudaStream_t est_stream(fmm_ctx* c);
+cudaEvent_t fork_event(fmm_ctx* c);
+cudaEvent_t join_event(fmm_ctx* c);
+Scratch& est_scratch(fmm_ctx* c);
+DevBuf<int>& est_stats(fmm_ctx* c);
+
+// one fmm! evaluation into out16 (device, original target order), queued on st.
+// For the relative error methods the influence estimate (src/fmm.jl:1189-1276), which
+// only the M2L needs, runs on a second stream concurrently with the near field and the
+// upward pass; the M2L waits for it.
 void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, double* out16, fmm_result* res,
-             bool is_estimate) {
-  cudaStream_t st = c->stream;
+             bool is_estimate, cudaStream_t st, Scratch& sc, DevBuf<int>& stats) {
   const int p = o.expansion_order;
   const bool lh = in.kind == FMM_POINT_VORTEX;
   const int64_t ls_s = o.leaf_size_source;
   const int64_t ls_t = o.leaf_size_target > 0 ? o.leaf_size_target : ls_s;
   const bool ps = o.scalar_potential != 0, gs = o.gradient != 0, hs = o.hessian != 0;
   const int64_t launches0 = g_launches;
-  cudaEvent_t ev[8] = {};
+  cudaEvent_t ev[8] = {}, eve[2] = {};
   const bool timing = c->timing && !is_estimate && res;
-  if (timing)
+  if (timing) {
     for (auto& e : ev) FMM_CUDA_TRY(cudaEventCreate(&e));
+    for (auto& e : eve) FMM_CUDA_TRY(cudaEventCreate(&e));
+  }
   auto mark = [&](int k) {
     if (timing) FMM_CUDA_TRY(cudaEventRecord(ev[k], st));
   };
@@ -193,7 +231,7 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   // ---- trees (src/tree.jl:3-122)
   DevTree& S = W.tree[1];
   unpack_bodies(S, in.src, in.n_s, in.d, in.kind, true, st);
-  build_tree(S, c->sc, st, ls_s, o.list_method, o.shrink_recenter != 0);
+  build_tree(S, sc, st, ls_s, o.list_method, o.shrink_recenter != 0);
   W.shared = (in.tpos == nullptr) && (ls_t == ls_s);
   if (!W.shared) {
     DevTree& T = W.tree[0];
@@ -201,17 +239,39 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
     int64_t stride = in.tpos ? in.t_stride : in.d;
     int64_t nt = in.tpos ? in.n_t : in.n_s;
     unpack_bodies(T, tp, nt, stride, 0, false, st);
-    build_tree(T, c->sc, st, ls_t, o.list_method, o.shrink_recenter != 0);
+    build_tree(T, sc, st, ls_t, o.list_method, o.shrink_recenter != 0);
   }
   DevTree& T = W.target();
   mark(1);
   // ---- interaction lists (src/interaction_list.jl:3-19, 183-213)
-  build_lists(W.lists, T, S, c->sc, st, ls_s, o.multipole_acceptance, o.farfield != 0, o.nearfield != 0,
+  build_lists(W.lists, T, S, sc, st, ls_s, o.multipole_acceptance, o.farfield != 0, o.nearfield != 0,
               o.self_induced != 0, o.list_method);
   mark(2);
-  // ---- relative error methods: influence estimate (src/fmm.jl:1193-1276)
   FMM_CUDA_TRY(cudaMemsetAsync(T.max_influence.ptr, 0, T.n_branches * sizeof(double), st));
-  if (o.error_method == FMM_POWER_RELATIVE_GRADIENT || o.error_method == FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT) {
+  const bool estimate =
+      o.error_method == FMM_POWER_RELATIVE_GRADIENT || o.error_method == FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT;
+  if (estimate) FMM_CUDA_TRY(cudaEventRecord(fork_event(c), st));
+  // ---- evaluation passes (src/fmm.jl:1028-1089): near field and upward pass
+  const int64_t NH4 = 4 * nh(p);
+  upload_tables(c->tables, p, st);
+  S.multipole.grow(NH4 * S.n_branches);
+  T.local.grow(NH4 * T.n_branches);
+  FMM_CUDA_TRY(cudaMemsetAsync(S.multipole.ptr, 0, NH4 * S.n_branches * sizeof(double), st));
+  FMM_CUDA_TRY(cudaMemsetAsync(T.local.ptr, 0, NH4 * T.n_branches * sizeof(double), st));
+  W.acc13.grow(13 * (size_t)T.n_bodies);
+  FMM_CUDA_TRY(cudaMemsetAsync(W.acc13.ptr, 0, 13 * T.n_bodies * sizeof(double), st));
+  stats.grow(8);
+  FMM_CUDA_TRY(cudaMemsetAsync(stats.ptr, 0, 8 * sizeof(int), st));
+  count_p2p_pairs(T, S, W.lists, reinterpret_cast<unsigned long long*>(stats.ptr + 4), st);
+  launch_p2p(T, S, W.lists, W.acc13.ptr, in.kind, ps, gs, hs, o.precision, st);
+  mark(3);
+  if (o.upward_pass) {
+    launch_p2m(S, p, in.kind, c->tables, st);
+    launch_m2m(S, p, lh, c->tables, st);
+  }
+  mark(4);
+  // ---- relative error methods: influence estimate on the second stream
+  if (estimate) {
     fmm_options e = o;
     e.leaf_size_source = 5;
     e.leaf_size_target = 5;
@@ -228,31 +288,18 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
     e.precision = o.precision;  // the mixed solve estimates with its FP32 near field
     int64_t nt = in.tpos ? in.n_t : in.n_s;
     c->est_out16.grow(16 * (size_t)nt);
-    run_fmm(c, c->est, in, e, c->est_out16.ptr, nullptr, true);
-    branch_max_influence(T, c->est_out16.ptr, st);
-  }
-  mark(3);
-  // ---- evaluation passes (src/fmm.jl:1028-1089)
-  const int64_t NH4 = 4 * nh(p);
-  upload_tables(c->tables, p, st);
-  S.multipole.grow(NH4 * S.n_branches);
-  T.local.grow(NH4 * T.n_branches);
-  FMM_CUDA_TRY(cudaMemsetAsync(S.multipole.ptr, 0, NH4 * S.n_branches * sizeof(double), st));
-  FMM_CUDA_TRY(cudaMemsetAsync(T.local.ptr, 0, NH4 * T.n_branches * sizeof(double), st));
-  W.acc13.grow(13 * (size_t)T.n_bodies);
-  FMM_CUDA_TRY(cudaMemsetAsync(W.acc13.ptr, 0, 13 * T.n_bodies * sizeof(double), st));
-  c->stats.grow(8);
-  FMM_CUDA_TRY(cudaMemsetAsync(c->stats.ptr, 0, 8 * sizeof(int), st));
-  count_p2p_pairs(T, S, W.lists, reinterpret_cast<unsigned long long*>(c->stats.ptr + 4), st);
-  launch_p2p(T, S, W.lists, W.acc13.ptr, in.kind, ps, gs, hs, o.precision, st);
-  mark(4);
-  if (o.upward_pass) {
-    launch_p2m(S, p, in.kind, c->tables, st);
-    launch_m2m(S, p, lh, c->tables, st);
+    cudaStream_t es = est_stream(c);
+    FMM_CUDA_TRY(cudaStreamWaitEvent(es, fork_event(c), 0));
+    if (timing) FMM_CUDA_TRY(cudaEventRecord(eve[0], es));
+    run_fmm(c, c->est, in, e, c->est_out16.ptr, nullptr, true, es, est_scratch(c), est_stats(c));
+    branch_max_influence(T, c->est_out16.ptr, es);
+    if (timing) FMM_CUDA_TRY(cudaEventRecord(eve[1], es));
+    FMM_CUDA_TRY(cudaEventRecord(join_event(c), es));
+    FMM_CUDA_TRY(cudaStreamWaitEvent(st, join_event(c), 0));
   }
   mark(5);
   if (o.horizontal_pass)
-    launch_m2l(T, S, W.lists, p, lh, o.error_method, o.error_tolerance, o.bonus_expansion, nullptr, c->stats.ptr,
+    launch_m2l(T, S, W.lists, p, lh, o.error_method, o.error_tolerance, o.bonus_expansion, nullptr, stats.ptr,
                c->tables, st);
   mark(6);
   if (o.downward_pass) {
@@ -266,7 +313,7 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   mark(7);
   if (res) {
     int h[6] = {0, 0, 0, 0, 0, 0};
-    FMM_CUDA_TRY(cudaMemcpyAsync(h, c->stats.ptr, 6 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    FMM_CUDA_TRY(cudaMemcpyAsync(h, stats.ptr, 6 * sizeof(int), cudaMemcpyDeviceToHost, st));
     FMM_CUDA_TRY(cudaStreamSynchronize(st));
     unsigned long long fl, pairs;
     std::memcpy(&fl, &h[2], 8);
@@ -287,18 +334,22 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
       for (int k = 0; k < 7; ++k) FMM_CUDA_TRY(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
       res->t_tree_ms = ms[0];
       res->t_lists_ms = ms[1];
-      res->t_influence_ms = ms[2];
-      res->t_nearfield_ms = ms[3];
-      res->t_upward_ms = ms[4];
-      res->t_horizontal_ms = ms[5];
+      res->t_nearfield_ms = ms[2];
+      res->t_upward_ms = ms[3];
+      res->t_horizontal_ms = ms[5];  // ms[4]: waiting for the influence estimate
       res->t_downward_ms = ms[6];
+      float me = 0.0f;
+      if (estimate) FMM_CUDA_TRY(cudaEventElapsedTime(&me, eve[0], eve[1]));
+      res->t_influence_ms = me;  // on its own stream, overlapping the near field and the upward pass
       float tot;
       FMM_CUDA_TRY(cudaEventElapsedTime(&tot, ev[0], ev[7]));
       res->t_total_ms = tot;
     }
   }
-  if (timing)
+  if (timing) {
     for (auto& e : ev) cudaEventDestroy(e);
+    for (auto& e : eve) cudaEventDestroy(e);
+  }
 }
 
 void check_options(const fmm_options& o) {
@@ -419,6 +470,14 @@ int fmm_ctx_destroy(fmm_ctx* c) {
     w->acc13.release();
   }
   release_scratch(c->sc);
+  release_scratch(c->est_sc);
+  c->est_stats.release();
+  if (c->est_stream) {
+    cudaStreamSynchronize(c->est_stream);
+    cudaStreamDestroy(c->est_stream);
+  }
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   c->tables.Hs.release();
   c->tables.zeta.release();
   c->tables.eta.release();
@@ -517,7 +576,7 @@ int fmm_solve(fmm_ctx* c, const fmm_target_system* target, const fmm_source_syst
       in.t_stride = target->stride;
     }
     c->out16.grow(16 * (size_t)in.n_t);
-    run_fmm(c, c->main, in, *opt, c->out16.ptr, result, false);
+    run_fmm(c, c->main, in, *opt, c->out16.ptr, result, false, c->stream, c->sc, c->stats);
     // write the target buffer (rows 1..3 = positions, 4..16 = phi, gradient, hessian)
     int mem = target->memory;
     double* dst = target->out;
@@ -652,7 +711,7 @@ int fmm_vjp(fmm_ctx* c, const fmm_target_system* target, const fmm_source_system
     }
     const double* dout = stage(c, c->stage_d, d_out, 16 * (size_t)nt, mem);
     c->out16.grow(16 * (size_t)nt);
-    run_fmm(c, c->main, in, of, c->out16.ptr, result, false);
+    run_fmm(c, c->main, in, of, c->out16.ptr, result, false, c->stream, c->sc, c->stats);
     // adjoint solve: sources at the targets with the cotangents as strengths, targets at the sources
     const int da = kind == FMM_POINT_SOURCE ? 5 : 7;
     c->adj_src.grow((size_t)da * nt);
@@ -670,7 +729,7 @@ int fmm_vjp(fmm_ctx* c, const fmm_target_system* target, const fmm_source_system
     ia.t_stride = self ? 0 : d;
     fmm_options oa = of;
     c->adj_out16.grow(16 * (size_t)ns);
-    run_fmm(c, c->main, ia, oa, c->adj_out16.ptr, nullptr, false);
+    run_fmm(c, c->main, ia, oa, c->adj_out16.ptr, nullptr, false, c->stream, c->sc, c->stats);
     // combine
     const size_t n_res = (size_t)sdim * ns + 3 * (size_t)ns + (self ? 0 : 3 * (size_t)nt);
     c->vjp_out.grow(n_res);
