@@ -300,7 +300,7 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   mark(5);
   if (o.horizontal_pass)
     launch_m2l(T, S, W.lists, p, lh, o.error_method, o.error_tolerance, o.bonus_expansion, nullptr, stats.ptr,
-               c->tables, st);
+               c->tables, o.precision, st);
   mark(6);
   if (o.downward_pass) {
     launch_l2l(T, p, lh, c->tables, st);

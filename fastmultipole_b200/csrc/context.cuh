@@ -104,9 +104,9 @@ void launch_m2m(DevTree& s, int p, bool lh, const DevTables& tb, cudaStream_t st
 bool launch_m2m_lane(DevTree& s, int p, bool lh, cudaStream_t st);
 bool launch_l2l_lane(DevTree& t, int p, bool lh, cudaStream_t st);
 bool launch_m2l_lane(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh, int em, double eps, int be,
-                     int* p_used, int* stats, cudaStream_t st);
+                     int* p_used, int* stats, int precision, cudaStream_t st);
 void launch_m2l(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh, int error_method, double eps,
-                int be, int* p_used, int* stats, const DevTables& tb, cudaStream_t st);
+                int be, int* p_used, int* stats, const DevTables& tb, int precision, cudaStream_t st);
 void launch_l2l(DevTree& t, int p, bool lh, const DevTables& tb, cudaStream_t st);
 void launch_l2p(DevTree& t, int p, bool lh, bool ps, bool gs, bool hs, double* acc13, cudaStream_t st);
 // unit operators over explicit pair lists (device arrays)

@@ -1027,7 +1027,7 @@ void launch_m2m(DevTree& s, int p, bool lh, const DevTables& tb, cudaStream_t st
 }
 
 void launch_m2l(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh, int em, double eps, int be,
-                int* p_used, int* stats, const DevTables& tb, cudaStream_t st) {
+                int* p_used, int* stats, const DevTables& tb, int precision, cudaStream_t st) {
   if (L.n_m2l_targets == 0) return;
   // stats: [0] = max order used, [1] = any tolerance missed, [2..3] = flop count (u64)
   M2LStats S{stats, stats + 1, reinterpret_cast<unsigned long long*>(stats + 2)};
@@ -1051,7 +1051,7 @@ void launch_m2l(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh,
     FMM_CUDA_TRY(cudaGetLastError());
     return;
   }
-  if (launch_m2l_lane(t, s, L, p, lh, em, eps, be, p_used, stats, st)) return;
+  if (launch_m2l_lane(t, s, L, p, lh, em, eps, be, p_used, stats, precision, st)) return;
   M2LLaunch f{t, s, L, p, em, be, eps, p_used, S, tab_of(tb), st};
   dispatch_slots(p, lh, f);
 }

@@ -46,6 +46,11 @@ constexpr unsigned kAll = 0xffffffffu;
 // a sum run to the kernel's maximum order past the degree (its inputs are zero).
 constexpr int kLenTPad = kLenT + kLaneMaxP + 1;
 __constant__ double c_HBz[kLenTPad], c_HAz[kLenTPad], c_HBe[kLenTPad], c_HAe[kLenTPad];
+// single-precision copies for the mixed path, and k! for its scaled coaxial step
+__constant__ float c_HBzF[kLenTPad], c_HAzF[kLenTPad], c_HBeF[kLenTPad], c_HAeF[kLenTPad];
+constexpr int kFact = 2 * kLaneMaxP + 2;
+__constant__ double c_fact[kFact];
+__constant__ float c_factF[kFact];
 __constant__ double c_Mt[kNhMax], c_Lt[kNhMax];
 
 __host__ __device__ constexpr int hi(int n, int m) { return n * (n + 1) / 2 + m; }
@@ -87,6 +92,19 @@ void ensure_lane_tables(cudaStream_t st) {
   FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAz, haz.data(), kLenTPad * 8, 0, cudaMemcpyHostToDevice, st));
   FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBe, hbe.data(), kLenTPad * 8, 0, cudaMemcpyHostToDevice, st));
   FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAe, hae.data(), kLenTPad * 8, 0, cudaMemcpyHostToDevice, st));
+  std::vector<float> fbz(hbz.begin(), hbz.end()), faz(haz.begin(), haz.end()), fbe(hbe.begin(), hbe.end()),
+      fae(hae.begin(), hae.end());
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBzF, fbz.data(), kLenTPad * 4, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAzF, faz.data(), kLenTPad * 4, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBeF, fbe.data(), kLenTPad * 4, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAeF, fae.data(), kLenTPad * 4, 0, cudaMemcpyHostToDevice, st));
+  std::vector<double> fact(kFact);
+  std::vector<float> factf(kFact);
+  fact[0] = 1.0;
+  for (int k = 1; k < kFact; ++k) fact[k] = fact[k - 1] * k;
+  for (int k = 0; k < kFact; ++k) factf[k] = (float)fact[k];
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_fact, fact.data(), kFact * 8, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_factF, factf.data(), kFact * 4, 0, cudaMemcpyHostToDevice, st));
   FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Mt, mt.data(), kNhMax * 8, 0, cudaMemcpyHostToDevice, st));
   FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Lt, lt.data(), kNhMax * 8, 0, cudaMemcpyHostToDevice, st));
   FMM_CUDA_TRY(cudaStreamSynchronize(st));
@@ -99,26 +117,41 @@ void ensure_lane_tables(cudaStream_t st) {
 // E, O, Z, and P_nu +- Q_nu is accumulated into every output at once through
 // column nu of A H w / 2.  Sums run to PMAX from one column base, so the table
 // entries are uniform constant reads at fixed offsets and no term is predicated.
-template <int PMAX, bool LOCAL>
-__device__ __forceinline__ void rot_y(int n, const double (&Xr)[PMAX + 1], const double (&Xi)[PMAX + 1], double cb,
-                                      double sb, double (&Yr)[PMAX + 1], double (&Yi)[PMAX + 1]) {
+template <bool LOCAL, class V>
+__device__ __forceinline__ V tab_b(int i) {
+  if constexpr (sizeof(V) == 8)
+    return LOCAL ? c_HBe[i] : c_HBz[i];
+  else
+    return LOCAL ? c_HBeF[i] : c_HBzF[i];
+}
+template <bool LOCAL, class V>
+__device__ __forceinline__ V tab_a(int i) {
+  if constexpr (sizeof(V) == 8)
+    return LOCAL ? c_HAe[i] : c_HAz[i];
+  else
+    return LOCAL ? c_HAeF[i] : c_HAzF[i];
+}
+
+template <int PMAX, bool LOCAL, class V = double>
+__device__ __forceinline__ void rot_y(int n, const V (&Xr)[PMAX + 1], const V (&Xi)[PMAX + 1], V cb, V sb,
+                                      V (&Yr)[PMAX + 1], V (&Yi)[PMAX + 1]) {
   const int t0 = lenT(n - 1), w = n + 1;
 #pragma unroll
-  for (int m = 0; m <= PMAX; ++m) Yr[m] = Yi[m] = 0.0;
-  double c = 1.0, s = 0.0;  // cos, sin (nu beta) by the reference's recurrence
+  for (int m = 0; m <= PMAX; ++m) Yr[m] = Yi[m] = V(0);
+  V c = V(1), s = V(0);  // cos, sin (nu beta) by the reference's recurrence
 #pragma unroll 1
   for (int nu = 0; nu <= n; ++nu) {
     if (nu > 0) {
-      const double cn = cb * c - sb * s;
-      const double sn = sb * c + cb * s;
+      const V cn = cb * c - sb * s;
+      const V sn = sb * c + cb * s;
       c = cn;
       s = sn;
     }
     const int col = t0 + nu * w;
-    double Er = 0, Ei = 0, Or = 0, Oi = 0;
+    V Er = 0, Ei = 0, Or = 0, Oi = 0;
 #pragma unroll
     for (int a = 1; a <= PMAX; ++a) {
-      const double h = LOCAL ? c_HBe[col + a] : c_HBz[col + a];
+      const V h = tab_b<LOCAL, V>(col + a);
       if (a & 1) {
         Or += h * Xr[a];
         Oi += h * Xi[a];
@@ -127,22 +160,22 @@ __device__ __forceinline__ void rot_y(int n, const double (&Xr)[PMAX + 1], const
         Ei += h * Xi[a];
       }
     }
-    const double h0 = LOCAL ? c_HBe[col] : c_HBz[col];
-    const double Zr = h0 * Xr[0], Zi = h0 * Xi[0];
-    const double sg = ((n + nu) & 1) ? -1.0 : 1.0;
-    const double S1r = Er - Or, S1i = Ei - Oi;
-    const double S3r = Er + Or, S3i = Ei + Oi;
-    const double S2r = Zr + S3r, S2i = -(Zi + S3i);
-    const double S4r = Zr + S1r, S4i = -(Zi + S1i);
-    const double A1r = S1r + sg * S2r, A1i = S1i + sg * S2i;
-    const double A3r = S3r + sg * S4r, A3i = S3i + sg * S4i;
-    const double ss = LOCAL ? -s : s;
-    const double Pr = c * A1r - ss * A1i, Pi = c * A1i + ss * A1r;
-    const double Qr = c * A3r + ss * A3i, Qi = c * A3i - ss * A3r;
-    const double Rpr = Pr + Qr, Rpi = Pi + Qi, Rmr = Pr - Qr, Rmi = Pi - Qi;
+    const V h0 = tab_b<LOCAL, V>(col);
+    const V Zr = h0 * Xr[0], Zi = h0 * Xi[0];
+    const V sg = ((n + nu) & 1) ? V(-1) : V(1);
+    const V S1r = Er - Or, S1i = Ei - Oi;
+    const V S3r = Er + Or, S3i = Ei + Oi;
+    const V S2r = Zr + S3r, S2i = -(Zi + S3i);
+    const V S4r = Zr + S1r, S4i = -(Zi + S1i);
+    const V A1r = S1r + sg * S2r, A1i = S1i + sg * S2i;
+    const V A3r = S3r + sg * S4r, A3i = S3i + sg * S4i;
+    const V ss = LOCAL ? -s : s;
+    const V Pr = c * A1r - ss * A1i, Pi = c * A1i + ss * A1r;
+    const V Qr = c * A3r + ss * A3i, Qi = c * A3i - ss * A3r;
+    const V Rpr = Pr + Qr, Rpi = Pi + Qi, Rmr = Pr - Qr, Rmi = Pi - Qi;
 #pragma unroll
     for (int m = 0; m <= PMAX; ++m) {
-      const double h = LOCAL ? c_HAe[col + m] : c_HAz[col + m];
+      const V h = tab_a<LOCAL, V>(col + m);
       Yr[m] += h * ((m & 1) ? Rmr : Rpr);
       Yi[m] += h * ((m & 1) ? Rmi : Rpi);
     }
@@ -334,6 +367,164 @@ __device__ __forceinline__ void back_degree(int n, double un, const Pair& q, con
   __syncwarp();
 }
 
+// ---- single precision (the mixed solve).  Degree n of the rotated multipole is
+// stored scaled by t^-n (t = |target centre - source centre|), M'(n, m) = M(n, m) / t^n,
+// which keeps the FP32 values of order q (sources lie within MAC * t of their centre):
+// the coaxial factor (n + n')! / t^(n+n'+1) becomes (n + n')! with t^-(n+1) applied to
+// the finished local coefficient in FP64.  The error control reads the same quantities
+// unscaled in FP64; accumulation is FP64.
+__device__ __forceinline__ float& MSf(float* Ms, int i, int c, int lane) { return Ms[(2 * i + c) * 32 + lane]; }
+__device__ __forceinline__ float MSfr(const float* Ms, int i, int c, int lane) { return Ms[(2 * i + c) * 32 + lane]; }
+
+// rotate_z + rotate_y of degree n into shared memory (scaled by sc = t^-n); returns the
+// multipole power of degree n; y0r, y1r, y1i: unscaled rotated coefficients (n, 0), (n, 1)
+template <int PMAX>
+__device__ __forceinline__ double fwd_degree_f(int n, const Pair& q, float* Ms, int lane, double sc, double& y0r,
+                                               double& y1r, double& y1i) {
+  float Xr[PMAX + 1], Xi[PMAX + 1];
+  double er = 1.0, ei = 0.0, pw = 0.0;
+  const int base = hi(n, 0);
+#pragma unroll
+  for (int a = 0; a <= PMAX; ++a) {
+    Xr[a] = Xi[a] = 0.0f;
+    if (a > n) continue;
+    const double2 u = __ldg(reinterpret_cast<const double2*>(q.src) + 2 * (base + a));
+    const double Nt = c_Mt[base + a];
+    pw += (u.x * u.x + u.y * u.y) * Nt * Nt;
+    Xr[a] = (float)((n == 0 ? u.x : u.x * er - u.y * ei) * sc);
+    Xi[a] = (float)((n == 0 ? u.y : u.x * ei + u.y * er) * sc);
+    const double t = er;
+    er = er * q.cph - ei * q.sph;
+    ei = t * q.sph + ei * q.cph;
+  }
+  float Yr[PMAX + 1], Yi[PMAX + 1];
+  rot_y<PMAX, false, float>(n, Xr, Xi, (float)q.cth, (float)q.sth, Yr, Yi);
+#pragma unroll
+  for (int m = 0; m <= PMAX; ++m) {
+    if (m > n) break;
+    MSf(Ms, base + m, 0, lane) = Yr[m];
+    MSf(Ms, base + m, 1, lane) = Yi[m];
+  }
+  const double us = 1.0 / sc;
+  y0r = Yr[0] * us;
+  y1r = Yr[1 % (PMAX + 1)] * us;
+  y1i = Yi[1 % (PMAX + 1)] * us;
+  return sqrt(pw);
+}
+
+// local error estimate of degree n (eps_local above) from the scaled rotated multipole;
+// tn1 = t^-(n+1)
+__device__ __forceinline__ double eps_local_f(int n, const Pair& q, const float* Ms, int lane, bool power,
+                                              double tn1) {
+  if (power) {
+    double a = 0.0;
+#pragma unroll 1
+    for (int m = 0; m <= n; ++m) {
+      double vr = 0, vi = 0;
+#pragma unroll 1
+      for (int np = m; np <= n; ++np) {
+        const double c = c_fact[n + np];
+        vr += c * MSfr(Ms, hi(np, m), 0, lane);
+        vi += c * MSfr(Ms, hi(np, m), 1, lane);
+      }
+      vr *= tn1;
+      vi *= tn1;
+      const double Nt = c_Lt[hi(n, m)];
+      a += (vr * vr + vi * vi) * Nt * Nt;
+    }
+    const double lphi = sqrt(a);
+    return 1.7320508075688772 * lphi * q.r_l_nm1 * q.nm1_fact_inv / c_Lt[hi(n, 0)];
+  }
+  double a0 = 0, b1r = 0, b1i = 0;
+#pragma unroll 1
+  for (int np = 0; np <= n; ++np) a0 += c_fact[n + np] * MSfr(Ms, hi(np, 0), 0, lane);
+#pragma unroll 1
+  for (int np = 1; np <= n; ++np) {
+    b1r += c_fact[n + np] * MSfr(Ms, hi(np, 1), 0, lane);
+    b1i += c_fact[n + np] * MSfr(Ms, hi(np, 1), 1, lane);
+  }
+  return (fabs(b1r * tn1) + fabs(b1i * tn1) + fabs(a0 * tn1)) * q.r_l_nm1 * q.nm1_fact_inv;
+}
+
+template <int PMAX>
+__device__ __forceinline__ void err_step_f(int n, Pair& q, const float* Ms, int lane, bool power, int be,
+                                           double pn_phi, double y0r, double y1r, double y1i, double tn1) {
+  const double Mn0_next = c_Mt[hi(n, 0)];
+  double eps_mp;
+  if (power)
+    eps_mp = 1.7320508075688772 * q.mp_phi * q.r_mp_inv_np2 * q.np1_fact / q.Mn0;
+  else
+    eps_mp = (sqrt(y1r * y1r + y1i * y1i) + fabs(y0r)) * q.np1_fact * q.r_mp_inv_np2;
+  if (eps_mp <= q.thr) {
+    const double eps_l = eps_local_f(n, q, Ms, lane, power, tn1);
+    if (eps_mp + eps_l * 2.0 <= q.thr) {
+      q.P = n - 1 + (be ? 1 : 0);
+      q.ok = true;
+      q.active = false;
+      return;
+    }
+  }
+  if (power || n < PMAX) {
+    q.r_l_nm1 *= q.r_l;
+    q.r_mp_inv_np2 *= q.r_mp_inv;
+    q.nm1_fact_inv /= n;
+    q.np1_fact *= n + 1;
+  }
+  if (power) {
+    q.mp_phi = pn_phi;
+    q.Mn0 = Mn0_next;
+  }
+}
+
+// degree n of the local expansion from the scaled rotated multipole: coaxial
+// translation with (n + n')!, rotate_y back and back_rotate_z in FP32, then t^-(n+1) and
+// the sum over the 32 lanes in FP64 (tn1 = t^-(n+1))
+template <int PMAX>
+__device__ __forceinline__ void back_degree_f(int n, const Pair& q, const float* Ms, double* stage, double* acc,
+                                              int lane, double tn1) {
+  const bool on = q.valid && n <= q.P;
+  float Xr[PMAX + 1], Xi[PMAX + 1];
+#pragma unroll
+  for (int m = 0; m <= PMAX; ++m) {
+    Xr[m] = Xi[m] = 0.0f;
+    if (m > n) continue;
+    float vr = 0, vi = 0;
+    const int top = on ? q.P : m - 1;
+#pragma unroll 1
+    for (int np = m; np <= top; ++np) {
+      const float c = c_factF[n + np];
+      vr += c * MSfr(Ms, hi(np, m), 0, lane);
+      vi += c * MSfr(Ms, hi(np, m), 1, lane);
+    }
+    Xr[m] = vr;
+    Xi[m] = vi;
+  }
+  float Yr[PMAX + 1], Yi[PMAX + 1];
+  rot_y<PMAX, true, float>(n, Xr, Xi, (float)q.cth, (float)q.sth, Yr, Yi);
+  float er = 1.0f, ei = 0.0f;
+  const float cph = (float)q.cph, sph = (float)q.sph;
+#pragma unroll
+  for (int m = 0; m <= PMAX; ++m) {
+    if (m > n) break;
+    const float cr = er, ci = -ei;
+    const float vr = n == 0 ? Yr[m] : Yr[m] * cr - Yi[m] * ci;
+    const float vi = n == 0 ? Yi[m] : Yr[m] * ci + Yi[m] * cr;
+    stage[(2 * m) * 33 + lane] = on ? vr * tn1 : 0.0;
+    stage[(2 * m + 1) * 33 + lane] = on ? vi * tn1 : 0.0;
+    const float t = er;
+    er = er * cph - ei * sph;
+    ei = t * sph + ei * cph;
+  }
+  __syncwarp();
+  if (lane < 2 * (n + 1)) {
+    double v = 0.0;
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) v += stage[lane * 33 + k];
+    acc[2 * hi(n, 0) + lane] += v;
+  }
+  __syncwarp();
+}
+
 __device__ __forceinline__ unsigned long long lane_pair_flops(int P) {
   // the reference's operation count: 4 [2 sum_n (n+1)(2n+1) + sum_n sum_m (P-m+1)]
   // closed forms: sum_n (n+1)(2n+1) = P(P+1)(2P+1)/3 + 3P(P+1)/2 + P+1, sum_m (P-m+1)^2 = (P+1)(P+2)(2P+3)/6
@@ -353,13 +544,15 @@ __device__ __forceinline__ double min_dist_1d(double dx, double rm, double rp) {
   return same * minabs(right, left);
 }
 
-template <int PMAX>
-__host__ __device__ constexpr size_t lane_smem_doubles() {
-  return (size_t)2 * hi(PMAX + 1, 0) * 32 + (size_t)2 * (PMAX + 1) * 33 + (size_t)2 * hi(PMAX + 1, 0);
+// bytes: rotated multipole [2 NH][32] (V), stage [2 (PMAX+1)][33] and accumulator [2 NH] (FP64)
+template <int PMAX, class V>
+__host__ __device__ constexpr size_t lane_smem_bytes() {
+  return (size_t)2 * hi(PMAX + 1, 0) * 32 * sizeof(V) +
+         ((size_t)2 * (PMAX + 1) * 33 + (size_t)2 * hi(PMAX + 1, 0)) * sizeof(double);
 }
 
 // one warp per CTA; warp b owns target tgt_list[b] and its sources src_of[off[b] .. off[b+1])
-template <int PMAX>
+template <int PMAX, class V>
 __global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_list, const int* __restrict__ off,
                                                  const int* __restrict__ src_of, double* __restrict__ local,
                                                  const double* __restrict__ multipole,
@@ -370,10 +563,13 @@ __global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_lis
                                                  int* __restrict__ st_fail,
                                                  unsigned long long* __restrict__ st_flops) {
   constexpr int NH = hi(PMAX + 1, 0);
+  constexpr bool F32 = sizeof(V) == 4;
   extern __shared__ double lane_smem[];
-  double* Ms = lane_smem;                            // [2 NH][32]
-  double* stage = Ms + 2 * NH * 32;                  // [2 (PMAX+1)][33]
+  double* stage = lane_smem;                         // [2 (PMAX+1)][33]
   double* acc = stage + 2 * (PMAX + 1) * 33;         // [2 NH]
+  V* MsV = reinterpret_cast<V*>(acc + 2 * NH);       // rotated multipole [2 NH][32]
+  double* Ms = reinterpret_cast<double*>(MsV);
+  float* Msf = reinterpret_cast<float*>(MsV);
   const int lane = threadIdx.x;
   const int b = blockIdx.x;
   const int t = tgt_list[b];
@@ -443,25 +639,40 @@ __global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_lis
     // degree 0 for every valid lane, then degree by degree while a lane is active
     // (error control) or up to PMAX (plain)
     q.active = q.valid;
+    double sc = 1.0;  // t^-n (single precision path)
 #pragma unroll 1
     for (int n = 0; n <= PMAX; ++n) {
       if (!__any_sync(kAll, q.active)) break;
       if (!q.active) continue;
-      if (n > 0) q.un *= n * q.rinv;
+      if (n > 0) {
+        q.un *= n * q.rinv;
+        sc *= q.rinv;
+      }
       double y0r, y1r, y1i;
-      const double pn_phi = fwd_degree<PMAX>(n, q, Ms, lane, y0r, y1r, y1i);
-      if (errc && n > 0) err_step<PMAX>(n, q, Ms, lane, power, be, pn_phi, y0r, y1r, y1i);
+      if constexpr (F32) {
+        const double pn_phi = fwd_degree_f<PMAX>(n, q, Msf, lane, sc, y0r, y1r, y1i);
+        if (errc && n > 0) err_step_f<PMAX>(n, q, Msf, lane, power, be, pn_phi, y0r, y1r, y1i, sc * q.rinv);
+      } else {
+        const double pn_phi = fwd_degree<PMAX>(n, q, Ms, lane, y0r, y1r, y1i);
+        if (errc && n > 0) err_step<PMAX>(n, q, Ms, lane, power, be, pn_phi, y0r, y1r, y1i);
+      }
     }
     q.active = false;  // error control: lanes still active reached PMAX (P = PMAX, tolerance missed)
     int pw = q.valid ? q.P : -1;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) pw = max(pw, __shfl_xor_sync(kAll, pw, o));
     __syncwarp();
-    double un = q.rinv;
+    double un = q.rinv, tn1 = q.rinv;  // n! / t^(n+1) and t^-(n+1)
 #pragma unroll 1
     for (int n = 0; n <= pw; ++n) {
-      if (n > 0) un *= n * q.rinv;
-      back_degree<PMAX>(n, un, q, Ms, stage, acc, lane);
+      if (n > 0) {
+        un *= n * q.rinv;
+        tn1 *= q.rinv;
+      }
+      if constexpr (F32)
+        back_degree_f<PMAX>(n, q, Msf, stage, acc, lane, tn1);
+      else
+        back_degree<PMAX>(n, un, q, Ms, stage, acc, lane);
     }
     if (q.valid) {
       if (p_used) p_used[l] = q.P;
@@ -486,18 +697,27 @@ __global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_lis
   }
 }
 
-template <int PMAX>
-void run_lane(DevTree& t, const DevTree& s, const DevLists& L, int em, double eps, int be, int* p_used, int* stats,
-              cudaStream_t st) {
-  const size_t sm = lane_smem_doubles<PMAX>() * sizeof(double);
+template <int PMAX, class V>
+void run_lane_v(DevTree& t, const DevTree& s, const DevLists& L, int em, double eps, int be, int* p_used, int* stats,
+                cudaStream_t st) {
+  const size_t sm = lane_smem_bytes<PMAX, V>();
   if (sm > 48 * 1024)
-    FMM_CUDA_TRY(cudaFuncSetAttribute(k_m2l_lane<PMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    FMM_CUDA_TRY(cudaFuncSetAttribute(k_m2l_lane<PMAX, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   note_launch();
-  k_m2l_lane<PMAX><<<(int)L.n_m2l_targets, 32, sm, st>>>(
+  k_m2l_lane<PMAX, V><<<(int)L.n_m2l_targets, 32, sm, st>>>(
       L.m2l_tgt.ptr, L.m2l_off.ptr, L.m2l_s.ptr, t.local.ptr, s.multipole.ptr, t.tcenter.ptr, t.tbox.ptr,
       t.tradius.ptr, t.max_influence.ptr, s.scenter.ptr, em, eps, be, p_used, stats, stats + 1,
       reinterpret_cast<unsigned long long*>(stats + 2));
   FMM_CUDA_TRY(cudaGetLastError());
+}
+
+template <int PMAX>
+void run_lane(DevTree& t, const DevTree& s, const DevLists& L, int em, double eps, int be, int* p_used, int* stats,
+              int precision, cudaStream_t st) {
+  if (precision == FMM_PRECISION_MIXED)
+    run_lane_v<PMAX, float>(t, s, L, em, eps, be, p_used, stats, st);
+  else
+    run_lane_v<PMAX, double>(t, s, L, em, eps, be, p_used, stats, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -865,7 +1085,7 @@ struct L2LLaneGo {
 }  // namespace
 
 bool launch_m2l_lane(DevTree& t, const DevTree& s, const DevLists& L, int p, bool lh, int em, double eps, int be,
-                     int* p_used, int* stats, cudaStream_t st) {
+                     int* p_used, int* stats, int precision, cudaStream_t st) {
   if (lh || p < 1 || p > kLaneMaxP) return false;
   if (L.n_m2l_targets == 0) return true;
   ensure_lane_tables(st);
@@ -879,18 +1099,18 @@ bool launch_m2l_lane(DevTree& t, const DevTree& s, const DevLists& L, int p, boo
     return true;
   }
   switch (p) {
-    case 1: run_lane<1>(t, s, L, em, eps, be, p_used, stats, st); break;
-    case 2: run_lane<2>(t, s, L, em, eps, be, p_used, stats, st); break;
-    case 3: run_lane<3>(t, s, L, em, eps, be, p_used, stats, st); break;
-    case 4: run_lane<4>(t, s, L, em, eps, be, p_used, stats, st); break;
-    case 5: run_lane<5>(t, s, L, em, eps, be, p_used, stats, st); break;
-    case 6: run_lane<6>(t, s, L, em, eps, be, p_used, stats, st); break;
-    case 7: run_lane<7>(t, s, L, em, eps, be, p_used, stats, st); break;
-    case 8: run_lane<8>(t, s, L, em, eps, be, p_used, stats, st); break;
-    case 9: run_lane<9>(t, s, L, em, eps, be, p_used, stats, st); break;
-    case 10: run_lane<10>(t, s, L, em, eps, be, p_used, stats, st); break;
-    case 11: run_lane<11>(t, s, L, em, eps, be, p_used, stats, st); break;
-    default: run_lane<12>(t, s, L, em, eps, be, p_used, stats, st); break;
+    case 1: run_lane<1>(t, s, L, em, eps, be, p_used, stats, precision, st); break;
+    case 2: run_lane<2>(t, s, L, em, eps, be, p_used, stats, precision, st); break;
+    case 3: run_lane<3>(t, s, L, em, eps, be, p_used, stats, precision, st); break;
+    case 4: run_lane<4>(t, s, L, em, eps, be, p_used, stats, precision, st); break;
+    case 5: run_lane<5>(t, s, L, em, eps, be, p_used, stats, precision, st); break;
+    case 6: run_lane<6>(t, s, L, em, eps, be, p_used, stats, precision, st); break;
+    case 7: run_lane<7>(t, s, L, em, eps, be, p_used, stats, precision, st); break;
+    case 8: run_lane<8>(t, s, L, em, eps, be, p_used, stats, precision, st); break;
+    case 9: run_lane<9>(t, s, L, em, eps, be, p_used, stats, precision, st); break;
+    case 10: run_lane<10>(t, s, L, em, eps, be, p_used, stats, precision, st); break;
+    case 11: run_lane<11>(t, s, L, em, eps, be, p_used, stats, precision, st); break;
+    default: run_lane<12>(t, s, L, em, eps, be, p_used, stats, precision, st); break;
   }
   return true;
 }
