@@ -49,14 +49,17 @@ struct Scratch {
   DevBuf<unsigned char> cub;            // CUB temporary storage
   DevBuf<unsigned long long> keys_a, keys_b;
   DevBuf<int> vals_a, vals_b, tmp_i, tmp_j, tmp_k;
-  DevBuf<int2> front_a, front_b;
-  DevBuf<int2> dir_raw, m2l_raw;        // unsorted list pairs of the traversal
-  DevBuf<int> cnt_a, cnt_b;             // per-pair output counts / offsets (3 ints each)
+  DevBuf<int2> front_a, front_b;        // traversal frontiers
+  DevBuf<int2> dir_raw, m2l_raw;        // list pairs of the traversal in arrival order
+  DevBuf<int> cnt_a, cnt_b;             // pairs per target (direct, M2L)
   DevBuf<int> counts;                   // small host-visible counters
   DevBuf<double> tmp_d;
   DevBuf<double> staging;               // raw caller buffers copied to HBM
   DevBuf<double> out16;                 // target buffer in original order
   DevBuf<int> flag;
+  std::vector<int> step_hint;           // frontier sizes of the previous list build (launch shapes)
+  // target rows of the lists: offsets of all targets, unsorted rows, row classes
+  DevBuf<int> row_off_a, row_off_b, row_tmp_a, row_tmp_b, row_cur, row_mid, row_big_b, row_big_e, row_big_r;
 };
 
 struct DevTables {

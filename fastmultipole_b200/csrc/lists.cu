@@ -4,16 +4,24 @@
 // pair, either records a P2P pair, records an M2L pair (multipole acceptance
 // criterion d^2 * mac^2 > (r_s + r_t)^2) or descends into the children of one
 // side, with three rule sets (Barba, SelfTuning, SelfTuningTreeStop).  Here the
-// same per-pair decision runs on a breadth-first frontier of pairs: every step
-// classifies the whole frontier, scans the output counts and writes the P2P
-// pairs, M2L pairs and the next frontier in order.  The decisions are the
-// reference's, with the same FP64 operations (-fmad=false), so the resulting
-// pair sets are identical; a stable radix sort by target then gives the
-// target-sorted lists of sort_by_target (src/interaction_list.jl:183-213).
-// Within one target the pairs are in frontier order (the reference's are in
-// depth-first order); every consumer of the lists is order independent up to
-// floating-point summation order.
+// same per-pair decision runs on a breadth-first frontier of pairs, one kernel
+// per step with no host round trip in between: a pair at step k has depth(t) +
+// depth(s) = k, so (levels of the target tree + levels of the source tree - 1)
+// steps exhaust the recursion.  Outputs and the next frontier take their slots
+// with warp-aggregated atomics, and the pairs of every target are counted.  The
+// decisions are the reference's, with the same FP64 operations (-fmad=false), so
+// the pair sets are identical.  A scan of the per-target counts, a scatter into
+// the target rows and a segmented sort of every row by source index then give
+// the target-sorted lists of sort_by_target (src/interaction_list.jl:183-213)
+// with a canonical order inside each target (the reference's is depth-first);
+// the result does not depend on the order in which the atomics were served.
+// The host synchronises twice per build: after the traversal (totals, capacity
+// check) and after the row compaction (row counts).
+#include <climits>
+
 #include <cub/cub.cuh>
+#include <cub/block/block_merge_sort.cuh>
+#include <cub/warp/warp_merge_sort.cuh>
 
 #include "context.cuh"
 
@@ -22,15 +30,6 @@ namespace fmmb {
 namespace {
 
 enum : int { A_NONE = 0, A_DIRECT = 1, A_M2L = 2, A_SPLIT_T = 3, A_SPLIT_S = 4 };
-
-struct Cnt3 {
-  int d, m, n;
-};
-struct Cnt3Sum {
-  __device__ __forceinline__ Cnt3 operator()(const Cnt3& a, const Cnt3& b) const {
-    return Cnt3{a.d + b.d, a.m + b.m, a.n + b.n};
-  }
-};
 
 struct TreeRef {
   const int* n_children;
@@ -94,103 +93,347 @@ __device__ int decide(const TreeRef& T, int t, const TreeRef& S, int s, const Ru
   return A_SPLIT_S;
 }
 
-__global__ void k_classify(const int2* __restrict__ front, int nf, TreeRef T, TreeRef S, Rule R, Cnt3* __restrict__ cnt) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k > nf) return;
-  if (k == nf) {
-    cnt[k] = Cnt3{0, 0, 0};
-    return;
-  }
-  int2 p = front[k];
-  int nn;
-  int a = decide(T, p.x, S, p.y, R, nn);
-  cnt[k] = Cnt3{a == A_DIRECT, a == A_M2L, nn};
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kMaxSteps = 64;  // frontier counters; a traversal takes levels_t + levels_s - 1 steps
+enum : int { C_DIR = kMaxSteps, C_M2L, C_FLAG, C_ROWS_DIR, C_ROWS_M2L = C_ROWS_DIR + 8, C_N = 128 };
+constexpr int kStepThreads = 256;
+constexpr int kStepMaxBlocks = 148 * 16;
+
+__global__ void k_root_pair(int2* front, int* ctr) {
+  front[0] = make_int2(0, 0);
+  ctr[0] = 1;
 }
 
-__global__ void k_emit(const int2* __restrict__ front, int nf, TreeRef T, TreeRef S, Rule R,
-                       const Cnt3* __restrict__ off, int2* __restrict__ dir, int dir_base, int2* __restrict__ m2l,
-                       int m2l_base, int2* __restrict__ next) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nf) return;
-  int2 p = front[k];
-  int nn;
-  int a = decide(T, p.x, S, p.y, R, nn);
-  Cnt3 o = off[k];
-  if (a == A_DIRECT) {
-    dir[dir_base + o.d] = p;
-  } else if (a == A_M2L) {
-    m2l[m2l_base + o.m] = p;
-  } else if (a == A_SPLIT_T) {
-    int c0 = T.child_start[p.x];
-    for (int c = 0; c < nn; ++c) next[o.n + c] = make_int2(c0 + c, p.y);
-  } else if (a == A_SPLIT_S) {
-    int c0 = S.child_start[p.y];
-    for (int c = 0; c < nn; ++c) next[o.n + c] = make_int2(p.x, c0 + c);
+// Add one to cnt[t] for the lanes that pass, one atomic per distinct target of the warp.
+__device__ __forceinline__ void count_targets(bool on, int t, int lane, int* __restrict__ cnt) {
+  const unsigned grp = __match_any_sync(kFull, on ? t : -1 - lane);
+  if (on && lane == __ffs(grp) - 1) atomicAdd(cnt + t, __popc(grp));
+}
+
+constexpr int kStepItems = 4;                              // pairs per thread and chunk
+constexpr int kStepChunk = kStepThreads * kStepItems;      // pairs per block and chunk
+
+// Step k of the traversal: every pair of the frontier (ctr[k] pairs) is decided;
+// direct and M2L pairs go to the raw lists and count for their target, split
+// pairs put their children into the next frontier (ctr[k + 1] pairs).  A block
+// takes the slots of a whole chunk with one atomic per counter.  Slots past a
+// capacity are not written and raise the flag, which stops the later steps (the
+// host grows the buffers and repeats).
+__global__ void __launch_bounds__(kStepThreads) k_step(const int2* __restrict__ fin, int2* __restrict__ fout, int k,
+                                                      TreeRef T, TreeRef S, Rule R, int2* __restrict__ rdir,
+                                                      int2* __restrict__ rm2l, int* __restrict__ cdir,
+                                                      int* __restrict__ cm2l, int* __restrict__ ctr, int cap_f,
+                                                      int cap_d, int cap_m) {
+  constexpr int NW = kStepThreads / 32;
+  __shared__ int wsum[3][NW];
+  __shared__ int bbase[3];
+  // after an overflow the frontier holds unwritten slots: the steps that follow do
+  // nothing, and the host grows the buffers and repeats the traversal
+  if (ctr[C_FLAG]) return;
+  const int n = min(ctr[k], cap_f);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  bool bad = false;
+  for (int c0 = blockIdx.x * kStepChunk; c0 < n; c0 += gridDim.x * kStepChunk) {
+    int2 p[kStepItems];
+    int a[kStepItems], nn[kStepItems];
+    int cd = 0, cm = 0, cf = 0;
+#pragma unroll
+    for (int r = 0; r < kStepItems; ++r) {
+      const int i = c0 + r * kStepThreads + threadIdx.x;
+      p[r] = make_int2(0, 0);
+      a[r] = A_NONE;
+      nn[r] = 0;
+      if (i < n) {
+        p[r] = fin[i];
+        a[r] = decide(T, p[r].x, S, p[r].y, R, nn[r]);
+      }
+      if (a[r] != A_SPLIT_T && a[r] != A_SPLIT_S) nn[r] = 0;
+      cd += a[r] == A_DIRECT;
+      cm += a[r] == A_M2L;
+      cf += nn[r];
+    }
+    // block exclusive scan of (cd, cm, cf)
+    int id = cd, im = cm, jf = cf;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int x = __shfl_up_sync(kFull, id, o), y = __shfl_up_sync(kFull, im, o), z = __shfl_up_sync(kFull, jf, o);
+      if (lane >= o) id += x, im += y, jf += z;
+    }
+    if (lane == 31) wsum[0][w] = id, wsum[1][w] = im, wsum[2][w] = jf;
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      int tot = 0;
+      for (int q = 0; q < NW; ++q) tot += wsum[threadIdx.x][q];
+      const int slot = threadIdx.x == 0 ? C_DIR : threadIdx.x == 1 ? C_M2L : k + 1;
+      bbase[threadIdx.x] = tot ? atomicAdd(ctr + slot, tot) : 0;
+    }
+    __syncthreads();
+    int od = bbase[0] + id - cd, om = bbase[1] + im - cm, of = bbase[2] + jf - cf;
+    for (int q = 0; q < w; ++q) od += wsum[0][q], om += wsum[1][q], of += wsum[2][q];
+#pragma unroll
+    for (int r = 0; r < kStepItems; ++r) {
+      if (a[r] == A_DIRECT) {
+        if (od < cap_d)
+          rdir[od] = p[r];
+        else
+          bad = true;
+        ++od;
+      } else if (a[r] == A_M2L) {
+        if (om < cap_m)
+          rm2l[om] = p[r];
+        else
+          bad = true;
+        ++om;
+      } else if (nn[r]) {
+        if (of + nn[r] > cap_f) {
+          bad = true;
+        } else if (a[r] == A_SPLIT_T) {
+          const int cs = T.child_start[p[r].x];
+          for (int c = 0; c < nn[r]; ++c) fout[of + c] = make_int2(cs + c, p[r].y);
+        } else {
+          const int cs = S.child_start[p[r].y];
+          for (int c = 0; c < nn[r]; ++c) fout[of + c] = make_int2(p[r].x, cs + c);
+        }
+        of += nn[r];
+      }
+      count_targets(a[r] == A_DIRECT, p[r].x, lane, cdir);
+      count_targets(a[r] == A_M2L, p[r].x, lane, cm2l);
+    }
+    __syncthreads();  // wsum / bbase are rewritten by the next chunk
+  }
+  if (bad) atomicOr(ctr + C_FLAG, 1);
+}
+
+// per target: (count << 32) | (count > 0), so that one exclusive scan gives both the
+// row offset (high word) and the row ordinal among the non-empty targets (low word)
+__global__ void k_pack_counts(const int* __restrict__ cnt, int n, unsigned long long* __restrict__ pk) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int c = cnt[t];
+    pk[t] = ((unsigned long long)(unsigned)c << 32) | (c > 0 ? 1ull : 0ull);
   }
 }
 
-__global__ void k_split(const int2* __restrict__ in, int n, int* __restrict__ t, int* __restrict__ s) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) {
-    t[k] = in[k].x;
-    s[k] = in[k].y;
+constexpr int kSmallRow = 256;  // rows up to this length: one warp each (merge sort in registers)
+constexpr int kMidRow = 4096;   // up to this length: one block each; longer: segmented radix sort
+constexpr int kMidClasses = 4;  // block sorts of 512, 1024, 2048 and 4096 keys
+constexpr int kRowCtr = 2 + kMidClasses;  // per list: rows, rows per block class, big rows
+
+__host__ __device__ constexpr int mid_class(int c) { return c <= 512 ? 0 : c <= 1024 ? 1 : c <= 2048 ? 2 : 3; }
+
+// offsets of all targets (off, n + 1), the CSR of the non-empty ones (tgt, roff),
+// and the rows too long for a warp sort: row ordinals per block class (mid, n + 1
+// per class) and the bounds of the longer rows (big)
+__global__ void k_rows(const int* __restrict__ cnt, const unsigned long long* __restrict__ ex, int n,
+                       int* __restrict__ off, int* __restrict__ tgt, int* __restrict__ roff, int* __restrict__ ctr,
+                       int* __restrict__ mid, int* __restrict__ big_b, int* __restrict__ big_e,
+                       int* __restrict__ big_r) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t <= n; t += gridDim.x * blockDim.x) {
+    const unsigned long long e = ex[t];
+    const int o = (int)(e >> 32), r = (int)(e & 0xffffffffu);
+    off[t] = o;
+    if (t < n) {
+      const int c = cnt[t];
+      if (c > 0) {
+        tgt[r] = t;
+        roff[r] = o;
+      }
+      if (c > kMidRow) {
+        const int q = atomicAdd(ctr + 1 + kMidClasses, 1);
+        big_b[q] = o;
+        big_e[q] = o + c;
+        big_r[q] = r;
+      } else if (c > kSmallRow) {
+        const int k = mid_class(c);
+        mid[(size_t)k * (n + 1) + atomicAdd(ctr + 1 + k, 1)] = r;
+      }
+    } else {
+      roff[r] = o;
+      ctr[0] = r;
+    }
   }
 }
 
-template <class T>
-void grow_keep_l(DevBuf<T>& b, size_t n, cudaStream_t st) {
-  if (n <= b.cap) return;
-  DevBuf<T> nb;
-  nb.grow(n);
-  if (b.ptr && b.cap) FMM_CUDA_TRY(cudaMemcpyAsync(nb.ptr, b.ptr, b.cap * sizeof(T), cudaMemcpyDeviceToDevice, st));
-  FMM_CUDA_TRY(cudaStreamSynchronize(st));
-  b.release();
-  b = nb;
-  nb.ptr = nullptr;
-  nb.cap = 0;
+// raw pairs into their target's row, sources only (order inside a row fixed by the
+// sort that follows); one cursor atomic per distinct target of a warp
+__global__ void k_scatter(const int2* __restrict__ raw, int n, const int* __restrict__ off, int* __restrict__ cursor,
+                          int* __restrict__ out_s) {
+  const int lane = threadIdx.x & 31;
+  for (int w0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); w0 < n; w0 += gridDim.x * blockDim.x) {
+    const int i = w0 + lane;
+    const bool on = i < n;
+    const int2 p = on ? raw[i] : make_int2(-1 - lane, 0);
+    const unsigned grp = __match_any_sync(kFull, p.x);
+    const int leader = __ffs(grp) - 1;
+    int b = 0;
+    if (on && lane == leader) b = atomicAdd(cursor + p.x, __popc(grp));
+    b = __shfl_sync(kFull, b, leader);
+    if (on) out_s[off[p.x] + b + __popc(grp & ((1u << lane) - 1u))] = p.y;
+  }
 }
 
-// stable sort of (target, source) pairs by target and the per-target CSR
-void finish_list(DevBuf<int2>& raw, int64_t n, int nbits, DevBuf<int>& out_t, DevBuf<int>& out_s,
-                 DevBuf<int>& tgt, DevBuf<int>& off, int64_t& n_targets, Scratch& sc, cudaStream_t st) {
-  out_t.grow(n + 1);
-  out_s.grow(n + 1);
-  if (n == 0) {
-    n_targets = 0;
-    tgt.grow(1);
-    off.grow(2);
-    FMM_CUDA_TRY(cudaMemsetAsync(off.ptr, 0, 2 * sizeof(int), st));
-    return;
+struct IntLess {
+  __device__ __forceinline__ bool operator()(int a, int b) const { return a < b; }
+};
+
+constexpr int kSortWarps = 8;
+
+// rows of 32 (ITEMS / 2) + 1 .. 32 ITEMS sources (1 .. 32 for ITEMS = 1): one warp per
+// row, sorted by source index
+template <int ITEMS>
+__global__ void __launch_bounds__(kSortWarps * 32) k_sort_warp(const int* __restrict__ tgt,
+                                                                const int* __restrict__ roff, int n_rows,
+                                                                const int* __restrict__ in, int* __restrict__ out_t,
+                                                                int* __restrict__ out_s) {
+  using WMS = cub::WarpMergeSort<int, ITEMS, 32>;
+  __shared__ typename WMS::TempStorage tmp[kSortWarps];
+  constexpr int lo = ITEMS == 1 ? 1 : 16 * ITEMS + 1, hi = 32 * ITEMS;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WMS ws(tmp[w]);
+  for (int r = blockIdx.x * kSortWarps + w; r < n_rows; r += gridDim.x * kSortWarps) {
+    const int b = roff[r], len = roff[r + 1] - b;
+    if (len < lo || len > hi) continue;
+    const int t = tgt[r];
+    if (len == 1) {
+      if (lane == 0) out_t[b] = t, out_s[b] = in[b];
+      continue;
+    }
+    int keys[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+      const int i = lane * ITEMS + j;
+      keys[j] = i < len ? in[b + i] : INT_MAX;
+    }
+    ws.Sort(keys, IntLess(), len, INT_MAX);
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+      const int i = lane * ITEMS + j;
+      if (i < len) out_t[b + i] = t, out_s[b + i] = keys[j];
+    }
+    __syncwarp();
   }
-  sc.tmp_i.grow(n);
-  sc.tmp_j.grow(n);
+}
+
+// rows of one block class: one block of THREADS x ITEMS keys per row
+template <int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) k_sort_block(const int* __restrict__ mid, const int* __restrict__ tgt,
+                                                      const int* __restrict__ roff, const int* __restrict__ in,
+                                                      int* __restrict__ out_t, int* __restrict__ out_s) {
+  using BMS = cub::BlockMergeSort<int, THREADS, ITEMS>;
+  __shared__ typename BMS::TempStorage tmp;
+  const int r = mid[blockIdx.x];
+  const int b = roff[r], len = roff[r + 1] - b, t = tgt[r];
+  int keys[ITEMS];
+#pragma unroll
+  for (int j = 0; j < ITEMS; ++j) {
+    const int i = threadIdx.x * ITEMS + j;
+    keys[j] = i < len ? in[b + i] : INT_MAX;
+  }
+  BMS(tmp).Sort(keys, IntLess(), len, INT_MAX);
+#pragma unroll
+  for (int j = 0; j < ITEMS; ++j) {
+    const int i = threadIdx.x * ITEMS + j;
+    if (i < len) out_t[b + i] = t, out_s[b + i] = keys[j];
+  }
+}
+
+// target column of the rows sorted by the segmented radix sort
+__global__ void k_fill_rows(const int* __restrict__ big_r, const int* __restrict__ tgt, const int* __restrict__ roff,
+                            int* __restrict__ out_t) {
+  const int r = big_r[blockIdx.x];
+  const int b = roff[r], e = roff[r + 1], t = tgt[r];
+  for (int i = b + threadIdx.x; i < e; i += blockDim.x) out_t[i] = t;
+}
+
+int blocks_for(int64_t n, int threads) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, kStepMaxBlocks));
+}
+
+// one list (direct or M2L) being turned into target rows
+struct RowBuild {
+  const int* cnt;
+  const int2* raw;
+  int n;
+  DevBuf<int>*out_t, *out_s, *tgt, *roff;
+  DevBuf<int>* off;
+  DevBuf<int>* tmp;
+  int* ctr;  // rows, rows per block class, big rows (kRowCtr ints)
+};
+
+// offsets and row CSR (before the host reads the row counts)
+void rows_of(RowBuild& B, int nt, Scratch& sc, cudaStream_t st) {
+  B.out_t->grow((size_t)B.n + 1);
+  B.out_s->grow((size_t)B.n + 1);
+  B.tgt->grow((size_t)nt + 1);
+  B.roff->grow((size_t)nt + 2);
+  B.off->grow((size_t)nt + 1);
+  sc.keys_a.grow((size_t)nt + 1);
+  sc.keys_b.grow((size_t)nt + 1);
   note_launch();
-  k_split<<<(int)((n + 255) / 256), 256, 0, st>>>(raw.ptr, (int)n, sc.tmp_i.ptr, sc.tmp_j.ptr);
+  k_pack_counts<<<blocks_for(nt + 1, 256), 256, 0, st>>>(B.cnt, nt + 1, sc.keys_a.ptr);
   size_t tb = 0;
-  unsigned int* ki = reinterpret_cast<unsigned int*>(sc.tmp_i.ptr);
-  unsigned int* ko = reinterpret_cast<unsigned int*>(out_t.ptr);
-  cub::DeviceRadixSort::SortPairs(nullptr, tb, ki, ko, sc.tmp_j.ptr, out_s.ptr, (int)n, 0, nbits, st);
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, sc.keys_a.ptr, sc.keys_b.ptr, nt + 1, st);
   sc.cub.grow(tb);
-  FMM_CUDA_TRY(cub::DeviceRadixSort::SortPairs(sc.cub.ptr, tb, ki, ko, sc.tmp_j.ptr, out_s.ptr, (int)n, 0, nbits, st));
-  // run-length encode the targets -> unique targets + counts -> offsets
-  tgt.grow(n + 1);
-  off.grow(n + 2);
-  sc.tmp_k.grow(n + 2);
-  sc.counts.grow(4);
-  tb = 0;
-  cub::DeviceRunLengthEncode::Encode(nullptr, tb, out_t.ptr, tgt.ptr, sc.tmp_k.ptr, sc.counts.ptr, (int)n, st);
-  sc.cub.grow(tb);
-  FMM_CUDA_TRY(cub::DeviceRunLengthEncode::Encode(sc.cub.ptr, tb, out_t.ptr, tgt.ptr, sc.tmp_k.ptr, sc.counts.ptr,
-                                                  (int)n, st));
-  int runs = 0;
-  FMM_CUDA_TRY(cudaMemcpyAsync(&runs, sc.counts.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
-  FMM_CUDA_TRY(cudaStreamSynchronize(st));
-  n_targets = runs;
-  FMM_CUDA_TRY(cudaMemsetAsync(sc.tmp_k.ptr + runs, 0, sizeof(int), st));
-  tb = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tb, sc.tmp_k.ptr, off.ptr, runs + 1, st);
-  sc.cub.grow(tb);
-  FMM_CUDA_TRY(cub::DeviceScan::ExclusiveSum(sc.cub.ptr, tb, sc.tmp_k.ptr, off.ptr, runs + 1, st));
+  FMM_CUDA_TRY(cub::DeviceScan::ExclusiveSum(sc.cub.ptr, tb, sc.keys_a.ptr, sc.keys_b.ptr, nt + 1, st));
+  note_launch();
+  k_rows<<<blocks_for(nt + 1, 256), 256, 0, st>>>(B.cnt, sc.keys_b.ptr, nt, B.off->ptr, B.tgt->ptr, B.roff->ptr,
+                                                  B.ctr, sc.row_mid.ptr, sc.row_big_b.ptr, sc.row_big_e.ptr,
+                                                  sc.row_big_r.ptr);
+  FMM_CUDA_TRY(cudaGetLastError());
+}
+
+// scatter into rows and sort every row by source index (after the host read the counts:
+// h = rows, rows per block class, big rows)
+void sort_rows(RowBuild& B, int nt, const int* h, int nbits, Scratch& sc, cudaStream_t st) {
+  if (B.n == 0) return;
+  const int rows = h[0], n_big = h[1 + kMidClasses];
+  B.tmp->grow((size_t)B.n + 1);
+  sc.row_cur.grow((size_t)nt + 1);
+  FMM_CUDA_TRY(cudaMemsetAsync(sc.row_cur.ptr, 0, (size_t)nt * sizeof(int), st));
+  note_launch();
+  k_scatter<<<blocks_for(B.n, 256), 256, 0, st>>>(B.raw, B.n, B.off->ptr, sc.row_cur.ptr, B.tmp->ptr);
+  const int gw = blocks_for((int64_t)rows * 32, kSortWarps * 32);
+  note_launch();
+  k_sort_warp<1><<<gw, kSortWarps * 32, 0, st>>>(B.tgt->ptr, B.roff->ptr, rows, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr);
+  note_launch();
+  k_sort_warp<2><<<gw, kSortWarps * 32, 0, st>>>(B.tgt->ptr, B.roff->ptr, rows, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr);
+  note_launch();
+  k_sort_warp<4><<<gw, kSortWarps * 32, 0, st>>>(B.tgt->ptr, B.roff->ptr, rows, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr);
+  note_launch();
+  k_sort_warp<8><<<gw, kSortWarps * 32, 0, st>>>(B.tgt->ptr, B.roff->ptr, rows, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr);
+  FMM_CUDA_TRY(cudaGetLastError());
+  const int* mid = sc.row_mid.ptr;
+  const size_t stride = (size_t)nt + 1;
+  if (h[1] > 0) {
+    note_launch();
+    k_sort_block<128, 4><<<h[1], 128, 0, st>>>(mid, B.tgt->ptr, B.roff->ptr, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr);
+  }
+  if (h[2] > 0) {
+    note_launch();
+    k_sort_block<256, 4><<<h[2], 256, 0, st>>>(mid + stride, B.tgt->ptr, B.roff->ptr, B.tmp->ptr, B.out_t->ptr,
+                                               B.out_s->ptr);
+  }
+  if (h[3] > 0) {
+    note_launch();
+    k_sort_block<256, 8><<<h[3], 256, 0, st>>>(mid + 2 * stride, B.tgt->ptr, B.roff->ptr, B.tmp->ptr, B.out_t->ptr,
+                                               B.out_s->ptr);
+  }
+  if (h[4] > 0) {
+    note_launch();
+    k_sort_block<256, 16><<<h[4], 256, 0, st>>>(mid + 3 * stride, B.tgt->ptr, B.roff->ptr, B.tmp->ptr, B.out_t->ptr,
+                                                B.out_s->ptr);
+  }
+  FMM_CUDA_TRY(cudaGetLastError());
+  if (n_big > 0) {
+    size_t tb = 0;
+    cub::DeviceSegmentedRadixSort::SortKeys(nullptr, tb, B.tmp->ptr, B.out_s->ptr, B.n, n_big, sc.row_big_b.ptr,
+                                            sc.row_big_e.ptr, 0, nbits, st);
+    sc.cub.grow(tb);
+    FMM_CUDA_TRY(cub::DeviceSegmentedRadixSort::SortKeys(sc.cub.ptr, tb, B.tmp->ptr, B.out_s->ptr, B.n, n_big,
+                                                         sc.row_big_b.ptr, sc.row_big_e.ptr, 0, nbits, st));
+    note_launch();
+    k_fill_rows<<<n_big, 256, 0, st>>>(sc.row_big_r.ptr, B.tgt->ptr, B.roff->ptr, B.out_t->ptr);
+    FMM_CUDA_TRY(cudaGetLastError());
+  }
 }
 
 }  // namespace
@@ -200,51 +443,83 @@ void build_lists(DevLists& L, const DevTree& tt, const DevTree& stt, Scratch& sc
   TreeRef T{tt.n_children.ptr, tt.child_start.ptr, tt.body_count.ptr, tt.tcenter.ptr, tt.tradius.ptr};
   TreeRef S{stt.n_children.ptr, stt.child_start.ptr, stt.body_count.ptr, stt.scenter.ptr, stt.sradius.ptr};
   Rule R{mac, leaf_size_source, method, ff, nf, si};
-
-  DevBuf<int2>& dir_raw = sc.dir_raw;
-  DevBuf<int2>& m2l_raw = sc.m2l_raw;
-  int64_t n_dir = 0, n_m2l = 0;
-  sc.front_a.grow(1024);
-  sc.front_b.grow(1024);
-  int2 root = make_int2(0, 0);
-  FMM_CUDA_TRY(cudaMemcpyAsync(sc.front_a.ptr, &root, sizeof(int2), cudaMemcpyHostToDevice, st));
-  int nfront = 1;
-  dir_raw.grow(std::max<size_t>(1024, (size_t)tt.n_leaves * 32));
-  m2l_raw.grow(std::max<size_t>(1024, (size_t)tt.n_branches * 64));
-  while (nfront > 0) {
-    sc.cnt_a.grow(3 * (size_t)(nfront + 1));
-    sc.cnt_b.grow(3 * (size_t)(nfront + 1));
-    Cnt3* cnt = reinterpret_cast<Cnt3*>(sc.cnt_a.ptr);
-    Cnt3* off = reinterpret_cast<Cnt3*>(sc.cnt_b.ptr);
-    int g = (nfront + 1 + 255) / 256;
+  const int nt = (int)tt.n_branches;
+  const int n_steps = tt.n_levels + stt.n_levels - 1;
+  FMM_CHECK(n_steps + 1 < kMaxSteps, FMM_ERR_TREE_DEPTH, "interaction-list traversal deeper than supported");
+  sc.counts.grow(C_N);
+  int* ctr = sc.counts.ptr;
+  sc.cnt_a.grow((size_t)nt + 1);
+  sc.cnt_b.grow((size_t)nt + 1);
+  // capacities: kept from earlier builds, grown when a traversal reports more
+  size_t cap_f = std::max<size_t>(4096, (size_t)nt * 32), cap_d = std::max<size_t>(4096, (size_t)tt.n_leaves * 64);
+  size_t cap_m = std::max<size_t>(4096, (size_t)nt * 96);
+  std::vector<int> h(C_N, 0);
+  for (int attempt = 0;; ++attempt) {
+    FMM_CHECK(attempt < 8, FMM_ERR_MEMORY, "interaction-list capacities did not converge");
+    sc.front_a.grow(cap_f);
+    sc.front_b.grow(cap_f);
+    sc.dir_raw.grow(cap_d);
+    sc.m2l_raw.grow(cap_m);
+    const int cf = (int)std::min<size_t>(sc.front_a.cap, sc.front_b.cap);
+    const int cd = (int)sc.dir_raw.cap, cm = (int)sc.m2l_raw.cap;
+    FMM_CUDA_TRY(cudaMemsetAsync(ctr, 0, C_N * sizeof(int), st));
+    FMM_CUDA_TRY(cudaMemsetAsync(sc.cnt_a.ptr, 0, ((size_t)nt + 1) * sizeof(int), st));
+    FMM_CUDA_TRY(cudaMemsetAsync(sc.cnt_b.ptr, 0, ((size_t)nt + 1) * sizeof(int), st));
     note_launch();
-    k_classify<<<g, 256, 0, st>>>(sc.front_a.ptr, nfront, T, S, R, cnt);
-    size_t tb = 0;
-    cub::DeviceScan::ExclusiveScan(nullptr, tb, cnt, off, Cnt3Sum(), Cnt3{0, 0, 0}, nfront + 1, st);
-    sc.cub.grow(tb);
-    FMM_CUDA_TRY(cub::DeviceScan::ExclusiveScan(sc.cub.ptr, tb, cnt, off, Cnt3Sum(), Cnt3{0, 0, 0},
-                                                nfront + 1, st));
-    Cnt3 tot;
-    FMM_CUDA_TRY(cudaMemcpyAsync(&tot, off + nfront, sizeof(Cnt3), cudaMemcpyDeviceToHost, st));
+    k_root_pair<<<1, 1, 0, st>>>(sc.front_a.ptr, ctr);
+    for (int k = 0; k < n_steps; ++k) {
+      const int2* fin = (k & 1) ? sc.front_b.ptr : sc.front_a.ptr;
+      int2* fout = (k & 1) ? sc.front_a.ptr : sc.front_b.ptr;
+      // grid from this scratch's previous build (the kernel strides over any frontier)
+      const int64_t hint = k < (int)sc.step_hint.size() ? sc.step_hint[k] : (int64_t)kStepChunk * kStepMaxBlocks;
+      note_launch();
+      k_step<<<blocks_for(hint + hint / 4 + 32, kStepChunk), kStepThreads, 0, st>>>(
+          fin, fout, k, T, S, R, sc.dir_raw.ptr, sc.m2l_raw.ptr, sc.cnt_a.ptr, sc.cnt_b.ptr, ctr, cf, cd, cm);
+      FMM_CUDA_TRY(cudaGetLastError());
+    }
+    FMM_CUDA_TRY(cudaMemcpyAsync(h.data(), ctr, C_N * sizeof(int), cudaMemcpyDeviceToHost, st));
     FMM_CUDA_TRY(cudaStreamSynchronize(st));
-    grow_keep_l(dir_raw, (size_t)(n_dir + tot.d + 1), st);
-    grow_keep_l(m2l_raw, (size_t)(n_m2l + tot.m + 1), st);
-    sc.front_b.grow((size_t)tot.n + 1);
-    note_launch();
-    k_emit<<<(nfront + 255) / 256, 256, 0, st>>>(sc.front_a.ptr, nfront, T, S, R, off, dir_raw.ptr, (int)n_dir,
-                                                 m2l_raw.ptr, (int)n_m2l, sc.front_b.ptr);
-    FMM_CUDA_TRY(cudaGetLastError());
-    n_dir += tot.d;
-    n_m2l += tot.m;
-    nfront = tot.n;
-    std::swap(sc.front_a, sc.front_b);
+    size_t max_f = 0;
+    for (int k = 0; k <= n_steps; ++k) max_f = std::max(max_f, (size_t)(unsigned)h[k]);
+    const size_t nd = (size_t)(unsigned)h[C_DIR], nm = (size_t)(unsigned)h[C_M2L];
+    if (h[C_FLAG] || max_f > (size_t)cf || nd > (size_t)cd || nm > (size_t)cm) {
+      // the counts after an overflow are partial: grow past them and at least double
+      cap_f = std::max(2 * (size_t)cf, max_f + max_f / 4 + 64);
+      cap_d = std::max(nd > (size_t)cd ? 2 * (size_t)cd : (size_t)cd, nd + nd / 4 + 64);
+      cap_m = std::max(nm > (size_t)cm ? 2 * (size_t)cm : (size_t)cm, nm + nm / 4 + 64);
+      continue;
+    }
+    FMM_CHECK(h[n_steps] == 0, FMM_ERR_TREE_DEPTH, "interaction-list traversal did not terminate");
+    sc.step_hint.assign(h.begin(), h.begin() + n_steps);
+    break;
   }
+  const int n_dir = h[C_DIR], n_m2l = h[C_M2L];
   int nbits = 1;
-  while ((1ll << nbits) <= tt.n_branches) ++nbits;
+  while ((1ll << nbits) <= stt.n_branches) ++nbits;
+  // the row classes of one list are built (k_rows) and consumed (sort_rows) before the
+  // next list's k_rows reuses the class arrays, so the lists take turns
+  sc.row_mid.grow((size_t)kMidClasses * (nt + 1));
+  sc.row_big_b.grow((size_t)nt + 1);
+  sc.row_big_e.grow((size_t)nt + 1);
+  sc.row_big_r.grow((size_t)nt + 1);
+  RowBuild lists[2] = {
+      {sc.cnt_a.ptr, sc.dir_raw.ptr, n_dir, &L.dir_t, &L.dir_s, &L.dir_tgt, &L.dir_off, &sc.row_off_a, &sc.row_tmp_a,
+       ctr + C_ROWS_DIR},
+      {sc.cnt_b.ptr, sc.m2l_raw.ptr, n_m2l, &L.m2l_t, &L.m2l_s, &L.m2l_tgt, &L.m2l_off, &sc.row_off_b, &sc.row_tmp_b,
+       ctr + C_ROWS_M2L}};
+  int rows[2] = {0, 0};
+  for (int q = 0; q < 2; ++q) {
+    rows_of(lists[q], nt, sc, st);
+    int hq[kRowCtr];
+    FMM_CUDA_TRY(cudaMemcpyAsync(hq, lists[q].ctr, kRowCtr * sizeof(int), cudaMemcpyDeviceToHost, st));
+    FMM_CUDA_TRY(cudaStreamSynchronize(st));
+    rows[q] = hq[0];
+    sort_rows(lists[q], nt, hq, nbits, sc, st);
+  }
   L.n_direct = n_dir;
   L.n_m2l = n_m2l;
-  finish_list(dir_raw, n_dir, nbits, L.dir_t, L.dir_s, L.dir_tgt, L.dir_off, L.n_dir_targets, sc, st);
-  finish_list(m2l_raw, n_m2l, nbits, L.m2l_t, L.m2l_s, L.m2l_tgt, L.m2l_off, L.n_m2l_targets, sc, st);
+  L.n_dir_targets = rows[0];
+  L.n_m2l_targets = rows[1];
 }
 
 }  // namespace fmmb
