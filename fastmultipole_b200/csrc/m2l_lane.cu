@@ -1013,12 +1013,152 @@ __global__ void __launch_bounds__(128) k_m2l_small(const int* __restrict__ tgt_l
   }
 }
 
+// Mixed-precision plain M2L at orders <= 3: the multipole is scaled by t^-n in FP64
+// and rotated in FP32; the coaxial translation runs in FP32 with (n + n')!, giving the
+// local coefficients times t^(n + 1), which are rotated back and accumulated in FP32
+// relative to the separation t0 of the target's first pair, out(n) += Y(n) (t0 / t)^(n + 1)
+// (the ratios stay far inside FP32 range); the lane shares are summed by shuffles and
+// scaled by t0^-(n + 1) in FP64 once per target.
 template <int P>
-void run_m2l_small(DevTree& t, const DevTree& s, const DevLists& L, int* p_used, int* stats, cudaStream_t st) {
+__global__ void __launch_bounds__(128) k_m2l_small_f(const int* __restrict__ tgt_list, const int* __restrict__ off,
+                                                     const int* __restrict__ src_of, int n_targets,
+                                                     double* __restrict__ local, const double* __restrict__ multipole,
+                                                     const double* __restrict__ tcen, const double* __restrict__ scen,
+                                                     int* __restrict__ p_used, int* __restrict__ st_pmax,
+                                                     unsigned long long* __restrict__ st_flops) {
+  constexpr int NH = hi(P + 1, 0);
+  const int lane = threadIdx.x & 31;
+  const int b = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (b >= n_targets) return;
+  const int t = tgt_list[b];
+  const double tc0 = tcen[3 * t], tc1 = tcen[3 * t + 1], tc2 = tcen[3 * t + 2];
+  const int l0 = off[b], l1 = off[b + 1];
+  double t0;
+  {
+    const int s = src_of[l0];
+    const double x = tc0 - scen[3 * s], y = tc1 - scen[3 * s + 1], z = tc2 - scen[3 * s + 2];
+    t0 = sqrt(x * x + y * y + z * z);
+  }
+  float accr[NH], acci[NH];
+#pragma unroll
+  for (int i = 0; i < NH; ++i) accr[i] = acci[i] = 0.f;
+  for (int l = l0 + lane; l < l1; l += 32) {
+    const int s = src_of[l];
+    const double* src = multipole + (int64_t)4 * NH * s;
+    const double xd = tc0 - scen[3 * s], yd = tc1 - scen[3 * s + 1], zd = tc2 - scen[3 * s + 2];
+    const float x = (float)xd, y = (float)yd, z = (float)zd;
+    const float rho2 = x * x + y * y, r2 = rho2 + z * z;
+    const float rinv = rsqrtf(r2);
+    float cph = 1.f, sph = 0.f, cth = z < 0.f ? -1.f : 1.f, sth = 0.f;
+    if (rho2 > 0.f) {
+      const float irho = rsqrtf(rho2);
+      cph = x * irho;
+      sph = y * irho;
+      cth = z * rinv;
+      sth = rho2 * irho * rinv;
+    }
+    const double tinv = (double)rinv;
+    float Mr[NH], Mi[NH];
+    double sn = 1.0;  // t^-n
+#pragma unroll
+    for (int n = 0; n <= P; ++n) {
+      if (n > 0) sn *= tinv;
+      float Xr[P + 1], Xi[P + 1], Yr[P + 1], Yi[P + 1];
+      float er = 1.f, ei = 0.f;
+#pragma unroll
+      for (int a = 0; a <= P; ++a) {
+        Xr[a] = Xi[a] = 0.f;
+        if (a > n) continue;
+        const double2 u = __ldg(reinterpret_cast<const double2*>(src) + 2 * (hi(n, 0) + a));
+        const float ur = (float)(u.x * sn), ui = (float)(u.y * sn);
+        Xr[a] = ur * er - ui * ei;
+        Xi[a] = ur * ei + ui * er;
+        const float tt = er;
+        er = er * cph - ei * sph;
+        ei = tt * sph + ei * cph;
+      }
+      rot_y<P, false, float>(n, Xr, Xi, cth, sth, Yr, Yi);
+#pragma unroll
+      for (int m = 0; m <= n; ++m) {
+        Mr[hi(n, m)] = Yr[m];
+        Mi[hi(n, m)] = Yi[m];
+      }
+    }
+    const float q = (float)(t0 * tinv);
+    float qn = 1.f;  // (t0 / t)^(n + 1)
+#pragma unroll
+    for (int n = 0; n <= P; ++n) {
+      qn *= q;
+      float Xr[P + 1], Xi[P + 1], Yr[P + 1], Yi[P + 1];
+#pragma unroll
+      for (int m = 0; m <= P; ++m) {
+        Xr[m] = Xi[m] = 0.f;
+        if (m > n) continue;
+        float vr = 0.f, vi = 0.f;
+#pragma unroll
+        for (int np = m; np <= P; ++np) {
+          const float c = c_factF[n + np];
+          vr += c * Mr[hi(np, m)];
+          vi += c * Mi[hi(np, m)];
+        }
+        Xr[m] = vr;
+        Xi[m] = vi;
+      }
+      rot_y<P, true, float>(n, Xr, Xi, cth, sth, Yr, Yi);
+      float er = 1.f, ei = 0.f;
+#pragma unroll
+      for (int m = 0; m <= n; ++m) {
+        const float vr = Yr[m] * er + Yi[m] * ei;  // times e^{-i m phi}
+        const float vi = Yi[m] * er - Yr[m] * ei;
+        accr[hi(n, m)] += vr * qn;
+        acci[hi(n, m)] += vi * qn;
+        const float tt = er;
+        er = er * cph - ei * sph;
+        ei = tt * sph + ei * cph;
+      }
+    }
+    if (p_used) p_used[l] = P;
+  }
+#pragma unroll
+  for (int i = 0; i < NH; ++i)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      accr[i] += __shfl_xor_sync(kAll, accr[i], o);
+      acci[i] += __shfl_xor_sync(kAll, acci[i], o);
+    }
+  double* dst = local + (int64_t)4 * NH * t;
+  const double t0inv = 1.0 / t0;
+  double sc = t0inv;  // t0^-(n + 1)
+#pragma unroll
+  for (int n = 0; n <= P; ++n) {
+    if (n > 0) sc *= t0inv;
+#pragma unroll
+    for (int m = 0; m <= n; ++m) {
+      const int i = hi(n, m);
+      if ((i & 31) == lane) {
+        dst[4 * i] += (double)accr[i] * sc;
+        dst[4 * i + 1] += (double)acci[i] * sc;
+      }
+    }
+  }
+  if (lane == 0) {
+    atomicMax(st_pmax, P);
+    atomicAdd(st_flops, (unsigned long long)(l1 - l0) * lane_pair_flops(P));
+  }
+}
+
+template <int P>
+void run_m2l_small(DevTree& t, const DevTree& s, const DevLists& L, int* p_used, int* stats, int precision,
+                   cudaStream_t st) {
   note_launch();
-  k_m2l_small<P><<<(int)((L.n_m2l_targets + 3) / 4), 128, 0, st>>>(
-      L.m2l_tgt.ptr, L.m2l_off.ptr, L.m2l_s.ptr, (int)L.n_m2l_targets, t.local.ptr, s.multipole.ptr, t.tcenter.ptr,
-      s.scenter.ptr, p_used, stats, reinterpret_cast<unsigned long long*>(stats + 2));
+  const int g = (int)((L.n_m2l_targets + 3) / 4);
+  auto* fl = reinterpret_cast<unsigned long long*>(stats + 2);
+  if (precision == FMM_PRECISION_MIXED)
+    k_m2l_small_f<P><<<g, 128, 0, st>>>(L.m2l_tgt.ptr, L.m2l_off.ptr, L.m2l_s.ptr, (int)L.n_m2l_targets, t.local.ptr,
+                                        s.multipole.ptr, t.tcenter.ptr, s.scenter.ptr, p_used, stats, fl);
+  else
+    k_m2l_small<P><<<g, 128, 0, st>>>(L.m2l_tgt.ptr, L.m2l_off.ptr, L.m2l_s.ptr, (int)L.n_m2l_targets, t.local.ptr,
+                                      s.multipole.ptr, t.tcenter.ptr, s.scenter.ptr, p_used, stats, fl);
   FMM_CUDA_TRY(cudaGetLastError());
 }
 
@@ -1091,11 +1231,11 @@ bool launch_m2l_lane(DevTree& t, const DevTree& s, const DevLists& L, int p, boo
   ensure_lane_tables(st);
   if (em == FMM_ERROR_NONE && p <= 3) {
     if (p == 1)
-      run_m2l_small<1>(t, s, L, p_used, stats, st);
+      run_m2l_small<1>(t, s, L, p_used, stats, precision, st);
     else if (p == 2)
-      run_m2l_small<2>(t, s, L, p_used, stats, st);
+      run_m2l_small<2>(t, s, L, p_used, stats, precision, st);
     else
-      run_m2l_small<3>(t, s, L, p_used, stats, st);
+      run_m2l_small<3>(t, s, L, p_used, stats, precision, st);
     return true;
   }
   switch (p) {

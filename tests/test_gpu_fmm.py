@@ -235,6 +235,29 @@ def test_mixed_precision_error_bounds(ctx):
     assert errs[1e-6, "mixed"] < 1.1 * errs[1e-6, "f64"] + 1e-7, errs
 
 
+def test_mixed_low_order_m2l_and_influence_match_f64(ctx):
+    # orders <= 3 (the influence estimate's order) run the single-precision M2L in the mixed
+    # path: the far field must agree with the FP64 solve to FP32 accuracy (1e-5 relative L2,
+    # far below the order-3 truncation error of ~1e-3), and the influence estimate of a
+    # relative error method (max_influence per target branch) to 1e-4
+    buf = clustered(40000, 13)
+    outs = {}
+    for prec in ("f64", "mixed"):
+        og = fm.make_options(expansion_order=3, leaf_size_source=20, multipole_acceptance=0.5, nearfield=False,
+                             scalar_potential=True, precision=prec)
+        outs[prec], res = fm.solve_buffers(buf, L.FMM_POINT_SOURCE, og, ctx=ctx)
+        assert res.n_m2l > 0
+    for rows in (slice(3, 4), slice(4, 7)):
+        assert rel_l2(outs["mixed"][:, rows], outs["f64"][:, rows]) < 1e-5
+    inf = {}
+    for prec in ("f64", "mixed"):
+        og = fm.make_options(expansion_order=8, leaf_size_source=40, multipole_acceptance=0.5,
+                             error_tolerance=fm.PowerRelativeGradient(1e-6), precision=prec)
+        fm.solve_buffers(buf, L.FMM_POINT_SOURCE, og, ctx=ctx)
+        inf[prec] = fm.get_tree(ctx, 0)["max_influence"]
+    np.testing.assert_allclose(inf["mixed"], inf["f64"], rtol=1e-4, atol=0)
+
+
 def test_python_api_systems(ctx):
     rng = np.random.default_rng(5)
     n = 4000
