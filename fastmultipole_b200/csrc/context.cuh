@@ -60,6 +60,9 @@ struct Scratch {
   std::vector<int> step_hint;           // frontier sizes of the previous list build (launch shapes)
   // target rows of the lists: offsets of all targets, unsorted rows, row classes
   DevBuf<int> row_off_a, row_off_b, row_tmp_a, row_tmp_b, row_cur, row_mid, row_big_b, row_big_e, row_big_r;
+  // branch records of the two trees for the traversal (centre + radius, counts)
+  DevBuf<double4> node_geo_t, node_geo_s;
+  DevBuf<int4> node_info_t, node_info_s;
 };
 
 struct DevTables {

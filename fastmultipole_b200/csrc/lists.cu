@@ -31,12 +31,11 @@ namespace {
 
 enum : int { A_NONE = 0, A_DIRECT = 1, A_M2L = 2, A_SPLIT_T = 3, A_SPLIT_S = 4 };
 
+// per branch of one tree in its role: centre and radius (target ones for the target
+// tree, source ones for the source tree), and (n_children, child_start, body_count)
 struct TreeRef {
-  const int* n_children;
-  const int* child_start;
-  const int* body_count;
-  const double* center;  // target centre (target tree) or source centre (source tree)
-  const double* radius;
+  const double4* geo;
+  const int4* info;
 };
 
 struct Rule {
@@ -46,33 +45,38 @@ struct Rule {
   bool ff, nf, si;
 };
 
-__device__ __forceinline__ bool mac_accept(const TreeRef& T, int t, const TreeRef& S, int s, double mac) {
-  double dx = T.center[3 * t] - S.center[3 * s];
-  double dy = T.center[3 * t + 1] - S.center[3 * s + 1];
-  double dz = T.center[3 * t + 2] - S.center[3 * s + 2];
+__device__ __forceinline__ bool mac_accept(const double4& tg, const double4& sg, double mac) {
+  double dx = tg.x - sg.x;
+  double dy = tg.y - sg.y;
+  double dz = tg.z - sg.z;
   double sep2 = dx * dx + dy * dy + dz * dz;
-  double summed = S.radius[s] + T.radius[t];
+  double summed = sg.w + tg.w;
   return sep2 * mac * mac > summed * summed;
 }
 
 // one step of build_interaction_lists! for the three rule sets
-// (src/interaction_list.jl:23-64, 66-120, 122-166)
-__device__ int decide(const TreeRef& T, int t, const TreeRef& S, int s, const Rule& R, int& n_next) {
+// (src/interaction_list.jl:23-64, 66-120, 122-166); for a split, n_next children
+// starting at child0 (of the target for A_SPLIT_T, of the source for A_SPLIT_S)
+__device__ int decide(const TreeRef& T, int t, const TreeRef& S, int s, const Rule& R, int& n_next, int& child0) {
   n_next = 0;
-  int nct = T.n_children[t], ncs = S.n_children[s];
-  int bt = T.body_count[t], bs = S.body_count[s];
+  child0 = 0;
+  const int4 ti = T.info[t], si = S.info[s];
+  const int nct = ti.x, ncs = si.x;
+  const int bt = ti.z, bs = si.z;
   bool both_leaves = (nct == 0) && (ncs == 0);
   bool dir_ok = (R.nf || (t == s && R.si)) && (t != s || R.si);
   if (R.method == FMM_LIST_BARBA) {
-    if (mac_accept(T, t, S, s, R.mac)) return R.ff ? A_M2L : A_NONE;
+    const double4 tg = T.geo[t], sg = S.geo[s];
+    if (mac_accept(tg, sg, R.mac)) return R.ff ? A_M2L : A_NONE;
     if (both_leaves) return dir_ok ? A_DIRECT : A_NONE;
     // target radius decides the side (src/interaction_list.jl:48)
-    double tr = T.radius[t], sr = S.radius[s];
-    if (ncs == 0 || (tr >= sr && nct != 0)) {
+    if (ncs == 0 || (tg.w >= sg.w && nct != 0)) {
       n_next = nct;
+      child0 = ti.y;
       return A_SPLIT_T;
     }
     n_next = ncs;
+    child0 = si.y;
     return A_SPLIT_S;
   }
   if (R.method == FMM_LIST_SELF_TUNING) {
@@ -80,17 +84,28 @@ __device__ int decide(const TreeRef& T, int t, const TreeRef& S, int s, const Ru
     fraction = fraction + (double)bs / (double)(R.ls * R.ls);
     fraction = fraction * (double)bt;
     if (fraction < 1.0 || both_leaves) return (R.nf && (t != s || R.si)) ? A_DIRECT : A_NONE;
-    if (mac_accept(T, t, S, s, R.mac)) return R.ff ? A_M2L : A_NONE;
+    if (mac_accept(T.geo[t], S.geo[s], R.mac)) return R.ff ? A_M2L : A_NONE;
   } else {  // SelfTuningTreeStop
     if (both_leaves) return dir_ok ? A_DIRECT : A_NONE;
-    if (mac_accept(T, t, S, s, R.mac)) return R.ff ? A_M2L : A_NONE;
+    if (mac_accept(T.geo[t], S.geo[s], R.mac)) return R.ff ? A_M2L : A_NONE;
   }
   if (ncs == 0 || (bt >= bs && nct != 0)) {
     n_next = nct;
+    child0 = ti.y;
     return A_SPLIT_T;
   }
   n_next = ncs;
+  child0 = si.y;
   return A_SPLIT_S;
+}
+
+__global__ void k_pack_nodes(int n, const double* __restrict__ center, const double* __restrict__ radius,
+                             const int* __restrict__ n_children, const int* __restrict__ child_start,
+                             const int* __restrict__ body_count, double4* __restrict__ geo, int4* __restrict__ info) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    geo[i] = make_double4(center[3 * i], center[3 * i + 1], center[3 * i + 2], radius[i]);
+    info[i] = make_int4(n_children[i], child_start[i], body_count[i], 0);
+  }
 }
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -135,7 +150,7 @@ __global__ void __launch_bounds__(kStepThreads) k_step(const int2* __restrict__ 
   bool bad = false;
   for (int c0 = blockIdx.x * kStepChunk; c0 < n; c0 += gridDim.x * kStepChunk) {
     int2 p[kStepItems];
-    int a[kStepItems], nn[kStepItems];
+    int a[kStepItems], nn[kStepItems], ch[kStepItems];
     int cd = 0, cm = 0, cf = 0;
 #pragma unroll
     for (int r = 0; r < kStepItems; ++r) {
@@ -143,9 +158,10 @@ __global__ void __launch_bounds__(kStepThreads) k_step(const int2* __restrict__ 
       p[r] = make_int2(0, 0);
       a[r] = A_NONE;
       nn[r] = 0;
+      ch[r] = 0;
       if (i < n) {
         p[r] = fin[i];
-        a[r] = decide(T, p[r].x, S, p[r].y, R, nn[r]);
+        a[r] = decide(T, p[r].x, S, p[r].y, R, nn[r], ch[r]);
       }
       if (a[r] != A_SPLIT_T && a[r] != A_SPLIT_S) nn[r] = 0;
       cd += a[r] == A_DIRECT;
@@ -188,11 +204,9 @@ __global__ void __launch_bounds__(kStepThreads) k_step(const int2* __restrict__ 
         if (of + nn[r] > cap_f) {
           bad = true;
         } else if (a[r] == A_SPLIT_T) {
-          const int cs = T.child_start[p[r].x];
-          for (int c = 0; c < nn[r]; ++c) fout[of + c] = make_int2(cs + c, p[r].y);
+          for (int c = 0; c < nn[r]; ++c) fout[of + c] = make_int2(ch[r] + c, p[r].y);
         } else {
-          const int cs = S.child_start[p[r].y];
-          for (int c = 0; c < nn[r]; ++c) fout[of + c] = make_int2(p[r].x, cs + c);
+          for (int c = 0; c < nn[r]; ++c) fout[of + c] = make_int2(p[r].x, ch[r] + c);
         }
         of += nn[r];
       }
@@ -440,10 +454,23 @@ void sort_rows(RowBuild& B, int nt, const int* h, int nbits, Scratch& sc, cudaSt
 
 void build_lists(DevLists& L, const DevTree& tt, const DevTree& stt, Scratch& sc, cudaStream_t st,
                  int64_t leaf_size_source, double mac, bool ff, bool nf, bool si, int method) {
-  TreeRef T{tt.n_children.ptr, tt.child_start.ptr, tt.body_count.ptr, tt.tcenter.ptr, tt.tradius.ptr};
-  TreeRef S{stt.n_children.ptr, stt.child_start.ptr, stt.body_count.ptr, stt.scenter.ptr, stt.sradius.ptr};
+  const int nt = (int)tt.n_branches, ns = (int)stt.n_branches;
+  sc.node_geo_t.grow((size_t)nt);
+  sc.node_info_t.grow((size_t)nt);
+  sc.node_geo_s.grow((size_t)ns);
+  sc.node_info_s.grow((size_t)ns);
+  note_launch();
+  k_pack_nodes<<<blocks_for(nt, 256), 256, 0, st>>>(nt, tt.tcenter.ptr, tt.tradius.ptr, tt.n_children.ptr,
+                                                     tt.child_start.ptr, tt.body_count.ptr, sc.node_geo_t.ptr,
+                                                     sc.node_info_t.ptr);
+  note_launch();
+  k_pack_nodes<<<blocks_for(ns, 256), 256, 0, st>>>(ns, stt.scenter.ptr, stt.sradius.ptr, stt.n_children.ptr,
+                                                     stt.child_start.ptr, stt.body_count.ptr, sc.node_geo_s.ptr,
+                                                     sc.node_info_s.ptr);
+  FMM_CUDA_TRY(cudaGetLastError());
+  TreeRef T{sc.node_geo_t.ptr, sc.node_info_t.ptr};
+  TreeRef S{sc.node_geo_s.ptr, sc.node_info_s.ptr};
   Rule R{mac, leaf_size_source, method, ff, nf, si};
-  const int nt = (int)tt.n_branches;
   const int n_steps = tt.n_levels + stt.n_levels - 1;
   FMM_CHECK(n_steps + 1 < kMaxSteps, FMM_ERR_TREE_DEPTH, "interaction-list traversal deeper than supported");
   sc.counts.grow(C_N);
