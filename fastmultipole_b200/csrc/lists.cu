@@ -111,7 +111,7 @@ __global__ void k_pack_nodes(int n, const double* __restrict__ center, const dou
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxSteps = 64;  // frontier counters; a traversal takes levels_t + levels_s - 1 steps
 enum : int { C_DIR = kMaxSteps, C_M2L, C_FLAG, C_ROWS_DIR, C_ROWS_M2L = C_ROWS_DIR + 8, C_N = 128 };
-constexpr int kStepThreads = 256;
+constexpr int kStepThreads = 128;
 constexpr int kStepMaxBlocks = 148 * 16;
 
 __global__ void k_root_pair(int2* front, int* ctr) {
