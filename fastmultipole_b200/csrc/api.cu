@@ -282,7 +282,9 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
     e.list_method = FMM_LIST_SELF_TUNING_TREE_STOP;
     e.farfield = e.nearfield = e.self_induced = 1;
     e.upward_pass = e.horizontal_pass = e.downward_pass = 1;
-    e.scalar_potential = 1;
+    // the relative error methods read only |grad| of the estimate (get_influence,
+    // src/fmm.jl:1180-1183): its potential, which the reference also computes, is skipped
+    e.scalar_potential = 0;
     e.gradient = 1;
     e.hessian = 0;
     e.precision = o.precision;  // the mixed solve estimates with its FP32 near field

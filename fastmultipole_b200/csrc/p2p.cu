@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
           ri.x = r2.x > 0.f ? rsqrt_ftz(r2.x) : 0.f;  // coincident bodies are skipped
           ri.y = r2.y > 0.f ? rsqrt_ftz(r2.y) : 0.f;
           const float2 qr = __fmul2_rn(make_float2(v.z, v.w), ri);
-          ph = __fadd2_rn(ph, qr);
+          if constexpr (PS) ph = __fadd2_rn(ph, qr);
           const float2 q3 = __fmul2_rn(__fmul2_rn(qr, ri), ri);
           gx = __ffma2_rn(dx, q3, gx);
           gy = __ffma2_rn(dy, q3, gy);
