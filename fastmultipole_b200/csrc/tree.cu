@@ -154,63 +154,74 @@ __device__ __forceinline__ bool exceeds(int n, int64_t ls, int method) {
   return fraction > 2.8284271247461903 && n > 1;
 }
 
+// The children of a splitting level-l branch are the runs of key digit l among its
+// bodies.  Eight lanes per branch: lane o finds where octant o starts (a binary search
+// over the branch's keys, in parallel instead of seven chained searches), lane o + 1
+// where it ends.
+constexpr unsigned kFullMask = 0xffffffffu;
+struct Octants {
+  int k;       // branch
+  int o;       // this lane's octant
+  bool split;  // the branch splits
+  int b, e;    // bodies of octant o: [b, e)
+  unsigned nonempty;  // bit q: octant q holds bodies (all lanes of the group)
+};
+__device__ __forceinline__ Octants octants_of(const unsigned long long* __restrict__ keys, int ls_node, int le_node,
+                                              int level, int64_t leaf_size, int method,
+                                              const int* __restrict__ body_start, const int* __restrict__ body_count,
+                                              int* __restrict__ err) {
+  Octants r;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  r.k = ls_node + (g >> 3);
+  r.o = g & 7;
+  const bool in = r.k < le_node;
+  const int cnt = in ? body_count[r.k] : 0;
+  r.split = in && exceeds(cnt, leaf_size, method);
+  if (r.split && level >= kMaxDepth) {
+    if (r.o == 0) atomicExch(err, 1);
+    r.split = false;
+  }
+  const int lo = r.split ? body_start[r.k] : 0, hi = lo + (r.split ? cnt : 0);
+  r.b = r.o == 0 ? lo : lower_bound_digit(keys, lo, hi, level, r.o);
+  const int nb = __shfl_down_sync(kFullMask, r.b, 1, 8);
+  r.e = r.o == 7 ? hi : nb;
+  const unsigned ball = __ballot_sync(kFullMask, r.split && r.e > r.b);
+  r.nonempty = (ball >> ((threadIdx.x & 31) & ~7)) & 0xffu;
+  return r;
+}
+
 __global__ void k_count_children(const unsigned long long* __restrict__ keys, int ls_node, int le_node, int level,
                                  int64_t leaf_size, int method, const int* __restrict__ body_start,
                                  const int* __restrict__ body_count, int* __restrict__ nch, int* __restrict__ err) {
-  int k = ls_node + blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= le_node) return;
-  int cnt = body_count[k];
-  int n = 0;
-  if (exceeds(cnt, leaf_size, method)) {
-    if (level >= kMaxDepth) {
-      atomicExch(err, 1);
-    } else {
-      // children of a level-l branch are the runs of key digit l
-      int lo = body_start[k], hi = lo + cnt;
-      int prev = lo;
-      for (int o = 1; o <= 8; ++o) {
-        int b = (o == 8) ? hi : lower_bound_digit(keys, prev, hi, level, o);
-        n += (b > prev);
-        prev = b;
-      }
-    }
-  }
-  nch[k - ls_node] = n;
+  const Octants r = octants_of(keys, ls_node, le_node, level, leaf_size, method, body_start, body_count, err);
+  if (r.k < le_node && r.o == 0) nch[r.k - ls_node] = __popc(r.nonempty);
 }
 
 __global__ void k_emit_children(const unsigned long long* __restrict__ keys, int ls_node, int le_node, int level,
-                                const int* __restrict__ nch, const int* __restrict__ off, int* body_start,
+                                int64_t leaf_size, int method, const int* __restrict__ off, int* body_start,
                                 int* body_count, int* child_start, int* n_children, int* parent, int* lev,
-                                double* gcenter, double* gbox, double* gradius) {
-  int k = ls_node + blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= le_node) return;
-  int j = off[k - ls_node];
-  int base = le_node + j;
-  int nc = nch[k - ls_node];
-  child_start[k] = base;
-  n_children[k] = nc;
-  if (nc == 0) return;
-  int lo = body_start[k], hi = lo + body_count[k];
-  double pc[3] = {gcenter[3 * k], gcenter[3 * k + 1], gcenter[3 * k + 2]};
-  double pbox = gbox[k], prad = gradius[k];
-  int prev = lo, c = base;
-  for (int o = 0; o < 8; ++o) {
-    int b = (o == 7) ? hi : lower_bound_digit(keys, prev, hi, level, o + 1);
-    if (b > prev) {
-      body_start[c] = prev;
-      body_count[c] = b - prev;
-      parent[c] = k;
-      lev[c] = level + 1;
-      double delta = pbox * 0.5;  // get_child_center: parent box is a cube of half width pbox
-      gcenter[3 * c] = pc[0] + ((o & 1) ? delta : -delta);
-      gcenter[3 * c + 1] = pc[1] + ((o & 2) ? delta : -delta);
-      gcenter[3 * c + 2] = pc[2] + ((o & 4) ? delta : -delta);
-      gbox[c] = pbox * 0.5;
-      gradius[c] = prad * 0.5;
-      ++c;
-    }
-    prev = b;
+                                double* gcenter, double* gbox, double* gradius, int* __restrict__ err) {
+  const Octants r = octants_of(keys, ls_node, le_node, level, leaf_size, method, body_start, body_count, err);
+  if (r.k >= le_node) return;
+  const int k = r.k, o = r.o;
+  const int base = le_node + off[k - ls_node];
+  if (o == 0) {
+    child_start[k] = base;
+    n_children[k] = __popc(r.nonempty);
   }
+  if (!((r.nonempty >> o) & 1u)) return;
+  const int c = base + __popc(r.nonempty & ((1u << o) - 1u));
+  const double pbox = gbox[k], prad = gradius[k];
+  body_start[c] = r.b;
+  body_count[c] = r.e - r.b;
+  parent[c] = k;
+  lev[c] = level + 1;
+  const double delta = pbox * 0.5;  // get_child_center: parent box is a cube of half width pbox
+  gcenter[3 * c] = gcenter[3 * k] + ((o & 1) ? delta : -delta);
+  gcenter[3 * c + 1] = gcenter[3 * k + 1] + ((o & 2) ? delta : -delta);
+  gcenter[3 * c + 2] = gcenter[3 * k + 2] + ((o & 4) ? delta : -delta);
+  gbox[c] = pbox * 0.5;
+  gradius[c] = prad * 0.5;
 }
 
 __global__ void k_root(const RootGeom* root, int64_t n, int* body_start, int* body_count, int* parent, int* lev,
@@ -507,7 +518,7 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
     int nl = le_node - ls_node;
     sc.tmp_i.grow(nl + 1);
     sc.tmp_j.grow(nl + 1);
-    int g = (nl + 127) / 128;
+    const int g = (int)((8ll * nl + 127) / 128);  // eight lanes per branch
     note_launch();
     k_count_children<<<g, 128, 0, st>>>(keys, ls_node, le_node, level, leaf_size, method, t.body_start.ptr,
                                         t.body_count.ptr, sc.tmp_i.ptr, sc.flag.ptr);
@@ -525,9 +536,10 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
     int total = h[0];
     ensure((size_t)le_node + total + 1);
     note_launch();
-    k_emit_children<<<g, 128, 0, st>>>(keys, ls_node, le_node, level, sc.tmp_i.ptr, sc.tmp_j.ptr, t.body_start.ptr,
-                                       t.body_count.ptr, t.child_start.ptr, t.n_children.ptr, t.parent.ptr,
-                                       t.level.ptr, t.gcenter.ptr, t.gbox.ptr, t.gradius.ptr);
+    k_emit_children<<<g, 128, 0, st>>>(keys, ls_node, le_node, level, leaf_size, method, sc.tmp_j.ptr,
+                                       t.body_start.ptr, t.body_count.ptr, t.child_start.ptr, t.n_children.ptr,
+                                       t.parent.ptr, t.level.ptr, t.gcenter.ptr, t.gbox.ptr, t.gradius.ptr,
+                                       sc.flag.ptr);
     FMM_CUDA_TRY(cudaGetLastError());
     if (total == 0) break;
     ls_node = le_node;
