@@ -244,8 +244,9 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   DevTree& T = W.target();
   mark(1);
   // ---- interaction lists (src/interaction_list.jl:3-19, 183-213)
+  // error-controlled M2L: rows ordered by separation, so that the 32 pairs of a pass stop at similar orders
   build_lists(W.lists, T, S, sc, st, ls_s, o.multipole_acceptance, o.farfield != 0, o.nearfield != 0,
-              o.self_induced != 0, o.list_method);
+              o.self_induced != 0, o.list_method, o.error_method != FMM_ERROR_NONE);
   mark(2);
   FMM_CUDA_TRY(cudaMemsetAsync(T.max_influence.ptr, 0, T.n_branches * sizeof(double), st));
   const bool estimate =

@@ -85,8 +85,11 @@ void unpack_bodies(DevTree& t, const double* dev_buf, int64_t n, int64_t stride,
 void branch_max_influence(DevTree& t, const double* out16_orig, cudaStream_t st);
 
 // ---- lists.cu ----
+// m2l_by_separation: M2L rows ordered by decreasing (r_s + r_t) / separation (pairs that
+// need similar expansion orders side by side), else every row by source index
 void build_lists(DevLists& L, const DevTree& tt, const DevTree& stt, Scratch& sc, cudaStream_t st,
-                 int64_t leaf_size_source, double mac, bool ff, bool nf, bool si, int method);
+                 int64_t leaf_size_source, double mac, bool ff, bool nf, bool si, int method,
+                 bool m2l_by_separation);
 
 // ---- p2p.cu ----
 // Near field over the direct list; accumulates into acc13 (sorted target order, 13 per body).

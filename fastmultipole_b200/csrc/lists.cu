@@ -11,10 +11,12 @@
 // with warp-aggregated atomics, and the pairs of every target are counted.  The
 // decisions are the reference's, with the same FP64 operations (-fmad=false), so
 // the pair sets are identical.  A scan of the per-target counts, a scatter into
-// the target rows and a segmented sort of every row by source index then give
-// the target-sorted lists of sort_by_target (src/interaction_list.jl:183-213)
-// with a canonical order inside each target (the reference's is depth-first);
-// the result does not depend on the order in which the atomics were served.
+// the target rows and a segmented sort of every row give the target-sorted lists
+// of sort_by_target (src/interaction_list.jl:183-213) with a canonical order inside
+// each target (the reference's is depth-first): by source index, or, for the M2L
+// rows of an error-controlled solve, by decreasing (r_s + r_t) / separation and then
+// source index, so that the pairs of one lane-per-pair pass stop at similar orders.
+// The result does not depend on the order in which the atomics were served.
 // The host synchronises twice per build: after the traversal (totals, capacity
 // check) and after the row compaction (row counts).
 #include <climits>
@@ -285,20 +287,47 @@ __global__ void k_scatter(const int2* __restrict__ raw, int n, const int* __rest
   }
 }
 
-struct IntLess {
-  __device__ __forceinline__ bool operator()(int a, int b) const { return a < b; }
+struct KeyLess {
+  __device__ __forceinline__ bool operator()(unsigned a, unsigned b) const { return a < b; }
 };
+
+// Sort key of a row entry: its source index, or, for M2L rows ordered by separation,
+// (4095 - q) << 20 | source with q = floor(4095 (r_s + r_t) / |c_t - c_s|) clamped to
+// [0, 4095]: the pairs of one target that need high expansion orders come first and
+// neighbouring pairs need similar orders (source indices < 2^20 on that path).
+constexpr int kSepShift = 20;
+struct RowKey {
+  const double4* sgeo;  // null: source order
+  double4 tg;
+  __device__ __forceinline__ unsigned enc(int s) const {
+    if (!sgeo) return (unsigned)s;
+    const double4 sg = sgeo[s];
+    const double dx = tg.x - sg.x, dy = tg.y - sg.y, dz = tg.z - sg.z;
+    const double rho = (sg.w + tg.w) / sqrt(dx * dx + dy * dy + dz * dz);
+    const int q = (int)fmin(4095.0, fmax(0.0, rho * 4095.0));
+    return ((unsigned)(4095 - q) << kSepShift) | (unsigned)s;
+  }
+  __device__ __forceinline__ int dec(unsigned k) const {
+    return sgeo ? (int)(k & ((1u << kSepShift) - 1u)) : (int)k;
+  }
+};
+__device__ __forceinline__ RowKey row_key(const double4* tgeo, const double4* sgeo, int t) {
+  RowKey k;
+  k.sgeo = sgeo;
+  k.tg = sgeo ? tgeo[t] : make_double4(0, 0, 0, 0);
+  return k;
+}
 
 constexpr int kSortWarps = 8;
 
-// rows of 32 (ITEMS / 2) + 1 .. 32 ITEMS sources (1 .. 32 for ITEMS = 1): one warp per
-// row, sorted by source index
+// rows of 32 (ITEMS / 2) + 1 .. 32 ITEMS entries (1 .. 32 for ITEMS = 1): one warp per row
 template <int ITEMS>
 __global__ void __launch_bounds__(kSortWarps * 32) k_sort_warp(const int* __restrict__ tgt,
                                                                 const int* __restrict__ roff, int n_rows,
                                                                 const int* __restrict__ in, int* __restrict__ out_t,
-                                                                int* __restrict__ out_s) {
-  using WMS = cub::WarpMergeSort<int, ITEMS, 32>;
+                                                                int* __restrict__ out_s, const double4* tgeo,
+                                                                const double4* sgeo) {
+  using WMS = cub::WarpMergeSort<unsigned, ITEMS, 32>;
   __shared__ typename WMS::TempStorage tmp[kSortWarps];
   constexpr int lo = ITEMS == 1 ? 1 : 16 * ITEMS + 1, hi = 32 * ITEMS;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -311,17 +340,18 @@ __global__ void __launch_bounds__(kSortWarps * 32) k_sort_warp(const int* __rest
       if (lane == 0) out_t[b] = t, out_s[b] = in[b];
       continue;
     }
-    int keys[ITEMS];
+    const RowKey rk = row_key(tgeo, sgeo, t);
+    unsigned keys[ITEMS];
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
       const int i = lane * ITEMS + j;
-      keys[j] = i < len ? in[b + i] : INT_MAX;
+      keys[j] = i < len ? rk.enc(in[b + i]) : UINT_MAX;
     }
-    ws.Sort(keys, IntLess(), len, INT_MAX);
+    ws.Sort(keys, KeyLess(), len, UINT_MAX);
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
       const int i = lane * ITEMS + j;
-      if (i < len) out_t[b + i] = t, out_s[b + i] = keys[j];
+      if (i < len) out_t[b + i] = t, out_s[b + i] = rk.dec(keys[j]);
     }
     __syncwarp();
   }
@@ -331,22 +361,24 @@ __global__ void __launch_bounds__(kSortWarps * 32) k_sort_warp(const int* __rest
 template <int THREADS, int ITEMS>
 __global__ void __launch_bounds__(THREADS) k_sort_block(const int* __restrict__ mid, const int* __restrict__ tgt,
                                                       const int* __restrict__ roff, const int* __restrict__ in,
-                                                      int* __restrict__ out_t, int* __restrict__ out_s) {
-  using BMS = cub::BlockMergeSort<int, THREADS, ITEMS>;
+                                                      int* __restrict__ out_t, int* __restrict__ out_s,
+                                                      const double4* tgeo, const double4* sgeo) {
+  using BMS = cub::BlockMergeSort<unsigned, THREADS, ITEMS>;
   __shared__ typename BMS::TempStorage tmp;
   const int r = mid[blockIdx.x];
   const int b = roff[r], len = roff[r + 1] - b, t = tgt[r];
-  int keys[ITEMS];
+  const RowKey rk = row_key(tgeo, sgeo, t);
+  unsigned keys[ITEMS];
 #pragma unroll
   for (int j = 0; j < ITEMS; ++j) {
     const int i = threadIdx.x * ITEMS + j;
-    keys[j] = i < len ? in[b + i] : INT_MAX;
+    keys[j] = i < len ? rk.enc(in[b + i]) : UINT_MAX;
   }
-  BMS(tmp).Sort(keys, IntLess(), len, INT_MAX);
+  BMS(tmp).Sort(keys, KeyLess(), len, UINT_MAX);
 #pragma unroll
   for (int j = 0; j < ITEMS; ++j) {
     const int i = threadIdx.x * ITEMS + j;
-    if (i < len) out_t[b + i] = t, out_s[b + i] = keys[j];
+    if (i < len) out_t[b + i] = t, out_s[b + i] = rk.dec(keys[j]);
   }
 }
 
@@ -371,6 +403,8 @@ struct RowBuild {
   DevBuf<int>* off;
   DevBuf<int>* tmp;
   int* ctr;  // rows, rows per block class, big rows (kRowCtr ints)
+  const double4* tgeo = nullptr;  // non-null: rows up to kMidRow ordered by separation (RowKey)
+  const double4* sgeo = nullptr;
 };
 
 // offsets and row CSR (before the host reads the row counts)
@@ -407,34 +441,39 @@ void sort_rows(RowBuild& B, int nt, const int* h, int nbits, Scratch& sc, cudaSt
   k_scatter<<<blocks_for(B.n, 256), 256, 0, st>>>(B.raw, B.n, B.off->ptr, sc.row_cur.ptr, B.tmp->ptr);
   const int gw = blocks_for((int64_t)rows * 32, kSortWarps * 32);
   note_launch();
-  k_sort_warp<1><<<gw, kSortWarps * 32, 0, st>>>(B.tgt->ptr, B.roff->ptr, rows, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr);
+  k_sort_warp<1><<<gw, kSortWarps * 32, 0, st>>>(B.tgt->ptr, B.roff->ptr, rows, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr,
+                                                  B.tgeo, B.sgeo);
   note_launch();
-  k_sort_warp<2><<<gw, kSortWarps * 32, 0, st>>>(B.tgt->ptr, B.roff->ptr, rows, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr);
+  k_sort_warp<2><<<gw, kSortWarps * 32, 0, st>>>(B.tgt->ptr, B.roff->ptr, rows, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr,
+                                                  B.tgeo, B.sgeo);
   note_launch();
-  k_sort_warp<4><<<gw, kSortWarps * 32, 0, st>>>(B.tgt->ptr, B.roff->ptr, rows, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr);
+  k_sort_warp<4><<<gw, kSortWarps * 32, 0, st>>>(B.tgt->ptr, B.roff->ptr, rows, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr,
+                                                  B.tgeo, B.sgeo);
   note_launch();
-  k_sort_warp<8><<<gw, kSortWarps * 32, 0, st>>>(B.tgt->ptr, B.roff->ptr, rows, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr);
+  k_sort_warp<8><<<gw, kSortWarps * 32, 0, st>>>(B.tgt->ptr, B.roff->ptr, rows, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr,
+                                                  B.tgeo, B.sgeo);
   FMM_CUDA_TRY(cudaGetLastError());
   const int* mid = sc.row_mid.ptr;
   const size_t stride = (size_t)nt + 1;
   if (h[1] > 0) {
     note_launch();
-    k_sort_block<128, 4><<<h[1], 128, 0, st>>>(mid, B.tgt->ptr, B.roff->ptr, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr);
+    k_sort_block<128, 4><<<h[1], 128, 0, st>>>(mid, B.tgt->ptr, B.roff->ptr, B.tmp->ptr, B.out_t->ptr, B.out_s->ptr,
+                                               B.tgeo, B.sgeo);
   }
   if (h[2] > 0) {
     note_launch();
     k_sort_block<256, 4><<<h[2], 256, 0, st>>>(mid + stride, B.tgt->ptr, B.roff->ptr, B.tmp->ptr, B.out_t->ptr,
-                                               B.out_s->ptr);
+                                               B.out_s->ptr, B.tgeo, B.sgeo);
   }
   if (h[3] > 0) {
     note_launch();
     k_sort_block<256, 8><<<h[3], 256, 0, st>>>(mid + 2 * stride, B.tgt->ptr, B.roff->ptr, B.tmp->ptr, B.out_t->ptr,
-                                               B.out_s->ptr);
+                                               B.out_s->ptr, B.tgeo, B.sgeo);
   }
   if (h[4] > 0) {
     note_launch();
     k_sort_block<256, 16><<<h[4], 256, 0, st>>>(mid + 3 * stride, B.tgt->ptr, B.roff->ptr, B.tmp->ptr, B.out_t->ptr,
-                                                B.out_s->ptr);
+                                                B.out_s->ptr, B.tgeo, B.sgeo);
   }
   FMM_CUDA_TRY(cudaGetLastError());
   if (n_big > 0) {
@@ -453,7 +492,8 @@ void sort_rows(RowBuild& B, int nt, const int* h, int nbits, Scratch& sc, cudaSt
 }  // namespace
 
 void build_lists(DevLists& L, const DevTree& tt, const DevTree& stt, Scratch& sc, cudaStream_t st,
-                 int64_t leaf_size_source, double mac, bool ff, bool nf, bool si, int method) {
+                 int64_t leaf_size_source, double mac, bool ff, bool nf, bool si, int method,
+                 bool m2l_by_separation) {
   const int nt = (int)tt.n_branches, ns = (int)stt.n_branches;
   sc.node_geo_t.grow((size_t)nt);
   sc.node_info_t.grow((size_t)nt);
@@ -534,6 +574,10 @@ void build_lists(DevLists& L, const DevTree& tt, const DevTree& stt, Scratch& sc
        ctr + C_ROWS_DIR},
       {sc.cnt_b.ptr, sc.m2l_raw.ptr, n_m2l, &L.m2l_t, &L.m2l_s, &L.m2l_tgt, &L.m2l_off, &sc.row_off_b, &sc.row_tmp_b,
        ctr + C_ROWS_M2L}};
+  if (m2l_by_separation && ns < (1 << kSepShift)) {
+    lists[1].tgeo = sc.node_geo_t.ptr;
+    lists[1].sgeo = sc.node_geo_s.ptr;
+  }
   int rows[2] = {0, 0};
   for (int q = 0; q < 2; ++q) {
     rows_of(lists[q], nt, sc, st);
