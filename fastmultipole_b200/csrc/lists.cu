@@ -144,9 +144,14 @@ __global__ void __launch_bounds__(kStepThreads) k_step(const int2* __restrict__ 
   constexpr int NW = kStepThreads / 32;
   __shared__ int wsum[3][NW];
   __shared__ int bbase[3];
+  __shared__ int stop;
   // after an overflow the frontier holds unwritten slots: the steps that follow do
-  // nothing, and the host grows the buffers and repeats the traversal
-  if (ctr[C_FLAG]) return;
+  // nothing, and the host grows the buffers and repeats the traversal.  Another block
+  // of this step may raise the flag meanwhile, so one thread reads it for the block:
+  // the block leaves or stays as a whole (its barriers and block sums need every warp)
+  if (threadIdx.x == 0) stop = *reinterpret_cast<volatile int*>(ctr + C_FLAG);
+  __syncthreads();
+  if (stop) return;
   const int n = min(ctr[k], cap_f);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   bool bad = false;
