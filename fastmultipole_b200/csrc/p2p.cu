@@ -221,6 +221,36 @@ __device__ __forceinline__ void pair1(R tx, R ty, R tz, R sx, R sy, R sz, R s0, 
   }
 }
 
+// One lane's slice of a packed batch on its two targets.  GUARD skips pairs with
+// r^2 = 0 (coincident bodies); without it such a pair makes the sums non-finite.
+template <bool GUARD, bool PS>
+__device__ __forceinline__ void packed_batch(const float4* __restrict__ B4, int j0, int nb, int SS, float2 tx2,
+                                             float2 ty2, float2 tz2, float2& ph, float2& gx, float2& gy, float2& gz) {
+#pragma unroll 4
+  for (int j = j0; j < nb; j += SS) {
+    const float4 u = B4[2 * j], v = B4[2 * j + 1];
+    const float2 dx = __fadd2_rn(tx2, make_float2(u.x, u.y));
+    const float2 dy = __fadd2_rn(ty2, make_float2(u.z, u.w));
+    const float2 dz = __fadd2_rn(tz2, make_float2(v.x, v.y));
+    float2 r2 = __fmul2_rn(dx, dx);
+    r2 = __ffma2_rn(dy, dy, r2);
+    r2 = __ffma2_rn(dz, dz, r2);
+    float2 ri;
+    if (GUARD) {
+      ri.x = r2.x > 0.f ? rsqrt_ftz(r2.x) : 0.f;
+      ri.y = r2.y > 0.f ? rsqrt_ftz(r2.y) : 0.f;
+    } else {
+      ri = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+    }
+    const float2 qr = __fmul2_rn(make_float2(v.z, v.w), ri);
+    if (PS) ph = __fadd2_rn(ph, qr);
+    const float2 q3 = __fmul2_rn(__fmul2_rn(qr, ri), ri);
+    gx = __ffma2_rn(dx, q3, gx);
+    gy = __ffma2_rn(dy, q3, gy);
+    gz = __ffma2_rn(dz, q3, gz);
+  }
+}
+
 template <class R, int KIND, bool PS, bool GS, bool HS>
 __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt_list, const int* __restrict__ off,
                                                      const int* __restrict__ src_of, const int* __restrict__ t_start,
@@ -270,11 +300,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
     while (lb < l1) {
       // candidate leaves lb + kWarps * lane; take the longest prefix that fits the batch
       const int l = lb + kWarps * lane;
-      int cnt = 0, sb = 0;
+      int cnt = 0, sb = 0, sl = -1;
       if (l < l1) {
-        int s = src_of[l];
-        sb = s_start[s];
-        cnt = s_count[s];
+        sl = src_of[l];
+        sb = s_start[sl];
+        cnt = s_count[sl];
       }
       if (lane == 0) {
         sb += poff;
@@ -298,6 +328,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
         lb += kWarps * nl;
         poff = 0;
       }
+      // the batch holds the target branch's own bodies (coincident pairs certain)
+      const bool self_batch = __any_sync(kAll, lane < nl && sl == t);
       // gather: body idx of the batch lies in candidate leaf k (largest k < nl with excl_k <= idx)
       for (int i0 = 0; i0 < nb; i0 += 32) {
         const int idx = i0 + lane;
@@ -339,24 +371,17 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
         const float2 ty2 = make_float2((float)ty[0], (float)ty[1]);
         const float2 tz2 = make_float2((float)tz[0], (float)tz[1]);
         float2 ph = make_float2(0.f, 0.f), gx = ph, gy = ph, gz = ph;
-#pragma unroll 4
-        for (int j = slice; j < nb; j += SS) {
-          const float4 u = B4[2 * j], v = B4[2 * j + 1];
-          const float2 dx = __fadd2_rn(tx2, make_float2(u.x, u.y));
-          const float2 dy = __fadd2_rn(ty2, make_float2(u.z, u.w));
-          const float2 dz = __fadd2_rn(tz2, make_float2(v.x, v.y));
-          float2 r2 = __fmul2_rn(dx, dx);
-          r2 = __ffma2_rn(dy, dy, r2);
-          r2 = __ffma2_rn(dz, dz, r2);
-          float2 ri;
-          ri.x = r2.x > 0.f ? rsqrt_ftz(r2.x) : 0.f;  // coincident bodies are skipped
-          ri.y = r2.y > 0.f ? rsqrt_ftz(r2.y) : 0.f;
-          const float2 qr = __fmul2_rn(make_float2(v.z, v.w), ri);
-          if constexpr (PS) ph = __fadd2_rn(ph, qr);
-          const float2 q3 = __fmul2_rn(__fmul2_rn(qr, ri), ri);
-          gx = __ffma2_rn(dx, q3, gx);
-          gy = __ffma2_rn(dy, q3, gy);
-          gz = __ffma2_rn(dz, q3, gz);
+        // pairs with r^2 = 0 (coincident bodies) are skipped: batches holding the target's own
+        // leaf guard every pair; the others run unguarded and, in the rare case that their sums
+        // come out non-finite, repeat the batch with the guard (the same result either way)
+        if (self_batch) {
+          packed_batch<true, PS>(B4, slice, nb, SS, tx2, ty2, tz2, ph, gx, gy, gz);
+        } else {
+          packed_batch<false, PS>(B4, slice, nb, SS, tx2, ty2, tz2, ph, gx, gy, gz);
+          if (!isfinite(ph.x + ph.y + gx.x + gx.y + gy.x + gy.y + gz.x + gz.y)) {
+            ph = gx = gy = gz = make_float2(0.f, 0.f);
+            packed_batch<true, PS>(B4, slice, nb, SS, tx2, ty2, tz2, ph, gx, gy, gz);
+          }
         }
         part[0][0] += (R)ph.x;
         part[1][0] += (R)ph.y;
