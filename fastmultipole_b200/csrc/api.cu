@@ -40,6 +40,16 @@ __global__ void k_unsort(const double* __restrict__ acc13, const int* __restrict
   }
 }
 
+// the influence estimate's output: |grad| of every body in the caller's order (the
+// one quantity the relative error methods read, get_influence, src/fmm.jl:1180-1183)
+__global__ void k_unsort_gradnorm(const double* __restrict__ acc13, const int* __restrict__ sort_index, int64_t n,
+                                  double* __restrict__ gnorm) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double* a = acc13 + 13 * i;
+    gnorm[sort_index ? sort_index[i] : i] = sqrt(a[1] * a[1] + a[2] * a[2] + a[3] * a[3]);
+  }
+}
+
 int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); }
 
 // out += in on rows 4..16 of the target buffer (rows 1..3 are the positions)
@@ -263,7 +273,7 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   FMM_CUDA_TRY(cudaMemsetAsync(W.acc13.ptr, 0, 13 * T.n_bodies * sizeof(double), st));
   stats.grow(8);
   FMM_CUDA_TRY(cudaMemsetAsync(stats.ptr, 0, 8 * sizeof(int), st));
-  count_p2p_pairs(T, S, W.lists, reinterpret_cast<unsigned long long*>(stats.ptr + 4), st);
+  if (res) count_p2p_pairs(T, S, W.lists, reinterpret_cast<unsigned long long*>(stats.ptr + 4), st);
   launch_p2p(T, S, W.lists, W.acc13.ptr, in.kind, ps, gs, hs, o.precision, st);
   mark(3);
   if (o.upward_pass) {
@@ -290,7 +300,7 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
     e.hessian = 0;
     e.precision = o.precision;  // the mixed solve estimates with its FP32 near field
     int64_t nt = in.tpos ? in.n_t : in.n_s;
-    c->est_out16.grow(16 * (size_t)nt);
+    c->est_out16.grow((size_t)nt);  // |grad| per body
     cudaStream_t es = est_stream(c);
     FMM_CUDA_TRY(cudaStreamWaitEvent(es, fork_event(c), 0));
     if (timing) FMM_CUDA_TRY(cudaEventRecord(eve[0], es));
@@ -311,7 +321,10 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   }
   // ---- unsort into the caller's order (buffer_to_target!, src/compatibility.jl:324-338)
   note_launch();
-  k_unsort<<<grid_for(T.n_bodies), 256, 0, st>>>(W.acc13.ptr, T.sort_index.ptr, T.pos.ptr, T.n_bodies, out16);
+  if (is_estimate)  // out16 receives |grad| per body (n doubles)
+    k_unsort_gradnorm<<<grid_for(T.n_bodies), 256, 0, st>>>(W.acc13.ptr, T.sort_index.ptr, T.n_bodies, out16);
+  else
+    k_unsort<<<grid_for(T.n_bodies), 256, 0, st>>>(W.acc13.ptr, T.sort_index.ptr, T.pos.ptr, T.n_bodies, out16);
   FMM_CUDA_TRY(cudaGetLastError());
   mark(7);
   if (res) {

@@ -81,8 +81,8 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
 // Unpack a caller buffer (body-major, stride doubles) into pos/str (original order).
 void unpack_bodies(DevTree& t, const double* dev_buf, int64_t n, int64_t stride, int n_strength,
                    bool has_radius, cudaStream_t st);
-// max_influence of every branch from |gradient| of the original bodies (16 per body).
-void branch_max_influence(DevTree& t, const double* out16_orig, cudaStream_t st);
+// max_influence of every branch from |gradient| of the original bodies (one per body, caller's order).
+void branch_max_influence(DevTree& t, const double* gnorm_orig, cudaStream_t st);
 
 // ---- lists.cu ----
 // m2l_by_separation: M2L rows ordered by decreasing (r_s + r_t) / separation (pairs that

@@ -292,28 +292,33 @@ __global__ void k_copy_geometry(int nb, const double* gcenter, const double* gbo
   tr[k] = sr[k] = gradius[k];
 }
 
+// min / max over an aligned group of G lanes (exact, so the grouping does not matter)
+template <int G = 32>
 __device__ __forceinline__ double wmin(double v) {
-  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = G / 2; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
+template <int G = 32>
 __device__ __forceinline__ double wmax(double v) {
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = G / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
 
-// shrink_leaf! (src/tree.jl:1141-1161): one warp per leaf
+// shrink_leaf! (src/tree.jl:1141-1161): a group of G lanes per leaf (32, or 8 when the
+// leaves hold a few bodies)
+template <int G>
 __global__ void k_shrink_leaves(const int* __restrict__ leaf_index, int n_leaves, const int* __restrict__ body_start,
                                 const int* __restrict__ body_count, const double4* __restrict__ pos, double* tc,
                                 double* sc, double* tr, double* sr, double* tb, double* sb) {
-  int lane = threadIdx.x & 31;
-  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= n_leaves) return;
-  int b = leaf_index[w];
-  int s = body_start[b], c = body_count[b];
+  const int lane = threadIdx.x & (G - 1);
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const bool valid = w < n_leaves;  // the groups past the end repeat the last leaf and write nothing
+  const int b = leaf_index[valid ? w : n_leaves - 1];
+  const int s = body_start[b], c = body_count[b];
   double4 p0 = pos[s];
   double tmn[3] = {p0.x, p0.y, p0.z}, tmx[3] = {p0.x, p0.y, p0.z};
   double smn[3] = {p0.x, p0.y, p0.z}, smx[3] = {p0.x, p0.y, p0.z};
-  for (int i = lane; i < c; i += 32) {
+  for (int i = lane; i < c; i += G) {
     double4 p = pos[s + i];
     double x[3] = {p.x, p.y, p.z};
     for (int d = 0; d < 3; ++d) {
@@ -325,15 +330,15 @@ __global__ void k_shrink_leaves(const int* __restrict__ leaf_index, int n_leaves
   }
   double tcen[3], scen[3];
   for (int d = 0; d < 3; ++d) {
-    tmn[d] = wmin(tmn[d]);
-    tmx[d] = wmax(tmx[d]);
-    smn[d] = wmin(smn[d]);
-    smx[d] = wmax(smx[d]);
+    tmn[d] = wmin<G>(tmn[d]);
+    tmx[d] = wmax<G>(tmx[d]);
+    smn[d] = wmin<G>(smn[d]);
+    smx[d] = wmax<G>(smx[d]);
     tcen[d] = (tmx[d] + tmn[d]) * 0.5;
     scen[d] = (smx[d] + smn[d]) * 0.5;
   }
   double trad = 0.0, srad = 0.0;
-  for (int i = lane; i < c; i += 32) {
+  for (int i = lane; i < c; i += G) {
     double4 p = pos[s + i];
     double dx = p.x - tcen[0], dy = p.y - tcen[1], dz = p.z - tcen[2];
     trad = fmax(trad, sqrt(dx * dx + dy * dy + dz * dz));
@@ -342,9 +347,9 @@ __global__ void k_shrink_leaves(const int* __restrict__ leaf_index, int n_leaves
     dz = p.z - scen[2];
     srad = fmax(srad, sqrt(dx * dx + dy * dy + dz * dz) + p.w);
   }
-  trad = wmax(trad);
-  srad = wmax(srad);
-  if (lane == 0) {
+  trad = wmax<G>(trad);
+  srad = wmax<G>(srad);
+  if (valid && lane == 0) {
     for (int d = 0; d < 3; ++d) {
       tc[3 * b + d] = tcen[d];
       sc[3 * b + d] = scen[d];
@@ -403,7 +408,7 @@ __global__ void k_shrink_branches(int l0, int l1, const int* __restrict__ child_
 // estimate_influence! tail (src/fmm.jl:1236-1262): max |grad| over each branch's bodies
 __global__ void k_leaf_maxinf(const int* __restrict__ leaf_index, int n_leaves, const int* __restrict__ body_start,
                               const int* __restrict__ body_count, const int* __restrict__ sort_index,
-                              const double* __restrict__ out16, double* __restrict__ mi) {
+                              const double* __restrict__ gnorm, double* __restrict__ mi) {
   int lane = threadIdx.x & 31;
   int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= n_leaves) return;
@@ -411,8 +416,7 @@ __global__ void k_leaf_maxinf(const int* __restrict__ leaf_index, int n_leaves, 
   int s = body_start[b], c = body_count[b];
   double m = 0.0;
   for (int i = lane; i < c; i += 32) {
-    const double* g = out16 + 16 * (int64_t)sort_index[s + i] + 4;
-    m = fmax(m, sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]));
+    m = fmax(m, gnorm[sort_index[s + i]]);
   }
   m = wmax(m);
   if (lane == 0) mi[b] = m;
@@ -612,9 +616,14 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
                                       t.tradius.ptr, t.sradius.ptr, t.tbox.ptr, t.sbox.ptr);
   if (shrink) {
     note_launch();
-    k_shrink_leaves<<<(int)((nleaves * 32ll + 255) / 256), 256, 0, st>>>(
-        t.leaf_index.ptr, nleaves, t.body_start.ptr, t.body_count.ptr, t.pos.ptr, t.tcenter.ptr, t.scenter.ptr,
-        t.tradius.ptr, t.sradius.ptr, t.tbox.ptr, t.sbox.ptr);
+    if (n <= 8 * (int64_t)nleaves)
+      k_shrink_leaves<8><<<(int)((nleaves * 8ll + 255) / 256), 256, 0, st>>>(
+          t.leaf_index.ptr, nleaves, t.body_start.ptr, t.body_count.ptr, t.pos.ptr, t.tcenter.ptr, t.scenter.ptr,
+          t.tradius.ptr, t.sradius.ptr, t.tbox.ptr, t.sbox.ptr);
+    else
+      k_shrink_leaves<32><<<(int)((nleaves * 32ll + 255) / 256), 256, 0, st>>>(
+          t.leaf_index.ptr, nleaves, t.body_start.ptr, t.body_count.ptr, t.pos.ptr, t.tcenter.ptr, t.scenter.ptr,
+          t.tradius.ptr, t.sradius.ptr, t.tbox.ptr, t.sbox.ptr);
     for (int l = t.n_levels - 1; l >= 0; --l) {
       int l0 = (int)t.levels_start[l], l1 = (int)t.levels_end[l];
       note_launch();
@@ -626,11 +635,11 @@ void build_tree(DevTree& t, Scratch& sc, cudaStream_t st, int64_t leaf_size, int
   FMM_CUDA_TRY(cudaGetLastError());
 }
 
-void branch_max_influence(DevTree& t, const double* out16_orig, cudaStream_t st) {
+void branch_max_influence(DevTree& t, const double* gnorm_orig, cudaStream_t st) {
   int nl = (int)t.n_leaves;
   note_launch();
   k_leaf_maxinf<<<(int)((nl * 32ll + 255) / 256), 256, 0, st>>>(t.leaf_index.ptr, nl, t.body_start.ptr,
-                                                                t.body_count.ptr, t.sort_index.ptr, out16_orig,
+                                                                t.body_count.ptr, t.sort_index.ptr, gnorm_orig,
                                                                 t.max_influence.ptr);
   for (int l = t.n_levels - 1; l >= 0; --l) {
     int l0 = (int)t.levels_start[l], l1 = (int)t.levels_end[l];
