@@ -626,10 +626,12 @@ __global__ void __launch_bounds__(32) k_op_p2m(const double4* __restrict__ pos, 
 constexpr int kL2PThreads = 128;
 constexpr int kCh = 13;  // channels: u, vx, vy, vz, h_xx..h_zz (column-major order)
 
-__device__ void l2p_coefficients(double* C, const double* __restrict__ L, int p, bool lh, bool ps, bool gs, bool hs) {
+// threads tid of nthr (the CTA, or a group of lanes of one warp when !cta) fill C
+__device__ void l2p_coefficients(double* C, const double* __restrict__ L, int p, bool lh, bool ps, bool gs, bool hs,
+                                 int tid, int nthr, bool cta) {
   // C[(ch * NH + i) * 2 + reim]
   const int NH = (p + 1) * (p + 2) / 2;
-  for (int i = threadIdx.x; i < NH; i += blockDim.x) {
+  for (int i = tid; i < NH; i += nthr) {
     int n, m;
     nm_of(i, n, m);
     double* c = C;
@@ -689,9 +691,12 @@ __device__ void l2p_coefficients(double* C, const double* __restrict__ L, int p,
       c[((1 + d) * NH + i) * 2 + 1] = gs ? V[2 * d + 1] : 0.0;
     }
   }
-  __syncthreads();
+  if (cta)
+    __syncthreads();
+  else
+    __syncwarp();
   // hessian channels from the velocity coefficients ("gradient_n_m"), n <= p-1
-  for (int i = threadIdx.x; i < NH; i += blockDim.x) {
+  for (int i = tid; i < NH; i += nthr) {
     int n, m;
     nm_of(i, n, m);
     double h[9][2];
@@ -786,7 +791,10 @@ __device__ void l2p_coefficients(double* C, const double* __restrict__ L, int p,
         C[(ch * NH + i) * 2 + 1] = h[3 * col + row][1];
       }
   }
-  __syncthreads();
+  if (cta)
+    __syncthreads();
+  else
+    __syncwarp();
 }
 
 // contract one body: regular harmonics by the reference's column recursion
@@ -858,10 +866,36 @@ __global__ void __launch_bounds__(kL2PThreads) k_l2p(const int* __restrict__ lea
                                                      double* __restrict__ acc13) {
   extern __shared__ double C[];
   const int b = leaf_index[blockIdx.x];
-  l2p_coefficients(C, L + 4 * nh(p) * b, p, lh != 0, ps != 0, gs != 0, hs != 0);
+  l2p_coefficients(C, L + 4 * nh(p) * b, p, lh != 0, ps != 0, gs != 0, hs != 0, threadIdx.x, blockDim.x, true);
   const int s0 = body_start[b], cnt = body_count[b];
   const double cx = tcen[3 * b], cy = tcen[3 * b + 1], cz = tcen[3 * b + 2];
   for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+    double4 x = pos[s0 + j];
+    l2p_body(C, p, x.x - cx, x.y - cy, x.z - cz, ps != 0, gs != 0, hs != 0, acc13 + 13 * (int64_t)(s0 + j));
+  }
+}
+
+// leaves of a few bodies: a group of 8 lanes per leaf, 16 leaves per CTA of 128 threads,
+// each group with its own coefficients in shared memory
+constexpr int kL2PGroup = 8, kL2PGroupThreads = 128;
+__global__ void __launch_bounds__(kL2PGroupThreads) k_l2p_group(const int* __restrict__ leaf_index, int n_leaves,
+                                                               const int* __restrict__ body_start,
+                                                               const int* __restrict__ body_count,
+                                                               const double* __restrict__ tcen,
+                                                               const double4* __restrict__ pos,
+                                                               const double* __restrict__ L, int p, int lh, int ps,
+                                                               int gs, int hs, double* __restrict__ acc13) {
+  extern __shared__ double Cg[];
+  const int g = threadIdx.x / kL2PGroup, lane = threadIdx.x % kL2PGroup;
+  const int leaf = blockIdx.x * (kL2PGroupThreads / kL2PGroup) + g;
+  const bool valid = leaf < n_leaves;  // groups past the end repeat the last leaf and write nothing
+  const int b = leaf_index[valid ? leaf : n_leaves - 1];
+  double* C = Cg + (size_t)g * kCh * 2 * nh(p);
+  l2p_coefficients(C, L + 4 * nh(p) * b, p, lh != 0, ps != 0, gs != 0, hs != 0, lane, kL2PGroup, false);
+  if (!valid) return;
+  const int s0 = body_start[b], cnt = body_count[b];
+  const double cx = tcen[3 * b], cy = tcen[3 * b + 1], cz = tcen[3 * b + 2];
+  for (int j = lane; j < cnt; j += kL2PGroup) {
     double4 x = pos[s0 + j];
     l2p_body(C, p, x.x - cx, x.y - cy, x.z - cz, ps != 0, gs != 0, hs != 0, acc13 + 13 * (int64_t)(s0 + j));
   }
@@ -871,7 +905,7 @@ __global__ void __launch_bounds__(kL2PThreads) k_op_l2p(int64_t n, const double*
                                                         const double* __restrict__ L, int p, int lh, int ps, int gs,
                                                         int hs, double* __restrict__ out13) {
   extern __shared__ double C[];
-  l2p_coefficients(C, L, p, lh != 0, ps != 0, gs != 0, hs != 0);
+  l2p_coefficients(C, L, p, lh != 0, ps != 0, gs != 0, hs != 0, threadIdx.x, blockDim.x, true);
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
     l2p_body(C, p, dx[3 * j], dx[3 * j + 1], dx[3 * j + 2], ps != 0, gs != 0, hs != 0, out13 + 13 * j);
 }
@@ -1065,13 +1099,22 @@ void launch_l2l(DevTree& t, int p, bool lh, const DevTables& tb, cudaStream_t st
 void launch_l2p(DevTree& t, int p, bool lh, bool ps, bool gs, bool hs, double* acc13, cudaStream_t st) {
   if (t.n_leaves == 0) return;
   size_t sm = l2p_smem(p);
-  allow_smem(k_l2p, sm);
   note_launch();
-  // leaves of a few bodies (on average <= 8) take one warp each instead of kL2PThreads threads
-  const int threads = t.n_bodies <= 8 * t.n_leaves ? 32 : kL2PThreads;
-  k_l2p<<<(int)t.n_leaves, threads, sm, st>>>(t.leaf_index.ptr, t.body_start.ptr, t.body_count.ptr,
-                                                   t.tcenter.ptr, t.pos.ptr, t.local.ptr, p, lh ? 1 : 0,
-                                                   ps ? 1 : 0, gs ? 1 : 0, hs ? 1 : 0, acc13);
+  const bool small = t.n_bodies <= 8 * t.n_leaves;
+  const size_t smg = (kL2PGroupThreads / kL2PGroup) * sm;
+  if (small && smg <= 96 * 1024) {
+    // leaves of a few bodies (on average <= 8), low orders: 8 lanes each, 16 per CTA
+    allow_smem(k_l2p_group, smg);
+    const int per = kL2PGroupThreads / kL2PGroup;
+    k_l2p_group<<<(int)((t.n_leaves + per - 1) / per), kL2PGroupThreads, smg, st>>>(
+        t.leaf_index.ptr, (int)t.n_leaves, t.body_start.ptr, t.body_count.ptr, t.tcenter.ptr, t.pos.ptr, t.local.ptr,
+        p, lh ? 1 : 0, ps ? 1 : 0, gs ? 1 : 0, hs ? 1 : 0, acc13);
+  } else {
+    allow_smem(k_l2p, sm);
+    k_l2p<<<(int)t.n_leaves, small ? 32 : kL2PThreads, sm, st>>>(t.leaf_index.ptr, t.body_start.ptr, t.body_count.ptr,
+                                                     t.tcenter.ptr, t.pos.ptr, t.local.ptr, p, lh ? 1 : 0, ps ? 1 : 0,
+                                                     gs ? 1 : 0, hs ? 1 : 0, acc13);
+  }
   FMM_CUDA_TRY(cudaGetLastError());
 }
 
