@@ -142,7 +142,9 @@ __device__ __forceinline__ void store(double* o, const A& acc, int k) {
 // 32 / TS slices along the batch, TS the smallest power of two that covers the
 // tile, so a leaf of 5 bodies keeps every lane busy as a leaf of 64 does.
 // Slices are summed by shuffles, warps through shared memory.  The mixed path
-// sums each batch in FP32 and the batches in FP64.
+// sums each batch in FP32 and the batches in FP64.  On the packed FP32 path, rows
+// of small target leaves (at most 8 bodies on average) take one warp each instead of
+// a CTA, so that the per-row setup and the cross-warp sum do not dominate their work.
 constexpr int kWarps = 4;
 constexpr int kTPT = 2;
 constexpr unsigned kAll = 0xffffffffu;
@@ -251,10 +253,13 @@ __device__ __forceinline__ void packed_batch(const float4* __restrict__ B4, int 
   }
 }
 
-template <class R, int KIND, bool PS, bool GS, bool HS>
+// RW: one warp per row (rows of small leaves, kWarps rows per CTA), the warp adding its
+// sums to the targets itself; otherwise one CTA per row, the warps splitting its sources.
+template <class R, int KIND, bool PS, bool GS, bool HS, bool RW>
 __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt_list, const int* __restrict__ off,
-                                                     const int* __restrict__ src_of, const int* __restrict__ t_start,
-                                                     const int* __restrict__ t_count, const double* __restrict__ t_center,
+                                                     int n_rows, const int* __restrict__ src_of,
+                                                     const int* __restrict__ t_start, const int* __restrict__ t_count,
+                                                     const double* __restrict__ t_center,
                                                      const int* __restrict__ s_start, const int* __restrict__ s_count,
                                                      const double4* __restrict__ tpos, const double4* __restrict__ spos,
                                                      const double4* __restrict__ sstr, double* __restrict__ acc13) {
@@ -267,8 +272,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   R* B = reinterpret_cast<R*>(p2p_smem) + w * NS * NB;  // this warp's batch, plane v at B[v * NB]
   double* red = reinterpret_cast<double*>(p2p_smem + kWarps * NS * NB * sizeof(R));  // [kWarps][32 kTPT][NA]
-  const int t = tgt_list[blockIdx.x];
-  const int l0 = off[blockIdx.x], l1 = off[blockIdx.x + 1];
+  const int row = RW ? blockIdx.x * kWarps + w : blockIdx.x;
+  if (RW && row >= n_rows) return;  // whole warps: no block barrier on the RW path
+  constexpr int LS = RW ? 1 : kWarps;  // stride of this warp's source leaves along the row
+  const int t = tgt_list[row];
+  const int l0 = off[row], l1 = off[row + 1];
   const int ts = t_start[t], tc = t_count[t];
   const double ox = MIXED ? t_center[3 * t] : 0.0;
   const double oy = MIXED ? t_center[3 * t + 1] : 0.0;
@@ -296,10 +304,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
     for (int k = 0; k < kTPT; ++k)
 #pragma unroll
       for (int a = 0; a < NA; ++a) part[k][a] = R(0), tot[k][a] = 0.0;
-    int lb = l0 + w, poff = 0;  // next source leaf of this warp, bodies of it already taken
+    int lb = l0 + (RW ? 0 : w), poff = 0;  // next source leaf of this warp, bodies of it already taken
     while (lb < l1) {
       // candidate leaves lb + kWarps * lane; take the longest prefix that fits the batch
-      const int l = lb + kWarps * lane;
+      const int l = lb + LS * lane;
       int cnt = 0, sb = 0, sl = -1;
       if (l < l1) {
         sl = src_of[l];
@@ -325,7 +333,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
         poff += NB;
       } else {
         nb = __shfl_sync(kAll, incl, nl - 1);
-        lb += kWarps * nl;
+        lb += LS * nl;
         poff = 0;
       }
       // the batch holds the target branch's own bodies (coincident pairs certain)
@@ -421,6 +429,22 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
       for (int k = 0; k < kTPT; ++k)
 #pragma unroll
         for (int a = 0; a < NA; ++a) tot[k][a] += __shfl_xor_sync(kAll, tot[k][a], o);
+    if constexpr (RW) {
+      // one warp owns the row: its sums go to the targets directly
+      if (slice == 0) {
+#pragma unroll
+        for (int k = 0; k < kTPT; ++k) {
+          const int i = ti + k * TS;
+          if (i < nt)
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+              if (KIND == FMM_POINT_SOURCE && a == 0 && !PS) continue;
+              atomicAdd(acc13 + 13 * (int64_t)(ts + tile + i) + chan_row<KIND, GS>(a), tot[k][a] * kOneOver4Pi);
+            }
+        }
+      }
+      continue;
+    }
     if (slice == 0) {
 #pragma unroll
       for (int k = 0; k < kTPT; ++k) {
@@ -512,13 +536,25 @@ template <class R, int KIND, bool PS, bool GS, bool HS>
 void run_p2p(const DevTree& tt, const DevTree& stt, const DevLists& L, double* acc13, cudaStream_t st) {
   if (L.n_dir_targets == 0) return;
   constexpr size_t smem = p2p_smem_bytes<R, KIND, GS, HS>();
-  if (smem > 48 * 1024)
-    FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2p<R, KIND, PS, GS, HS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
+  const int rows = (int)L.n_dir_targets;
   note_launch();
-  k_p2p<R, KIND, PS, GS, HS><<<(int)L.n_dir_targets, kWarps * 32, smem, st>>>(
-      L.dir_tgt.ptr, L.dir_off.ptr, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
-      stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13);
+  // target leaves of a few bodies (on average <= 8), packed FP32 kernel: one warp per row
+  // (measured slower for the FP64 kernel, whose rows keep a CTA each)
+  if (packed<R, KIND>() && tt.n_bodies <= 8 * tt.n_leaves) {
+    if (smem > 48 * 1024)
+      FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2p<R, KIND, PS, GS, HS, true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_p2p<R, KIND, PS, GS, HS, true><<<(rows + kWarps - 1) / kWarps, kWarps * 32, smem, st>>>(
+        L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
+        stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13);
+  } else {
+    if (smem > 48 * 1024)
+      FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2p<R, KIND, PS, GS, HS, false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_p2p<R, KIND, PS, GS, HS, false><<<rows, kWarps * 32, smem, st>>>(
+        L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
+        stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13);
+  }
   FMM_CUDA_TRY(cudaGetLastError());
 }
 
