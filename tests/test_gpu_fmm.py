@@ -258,6 +258,21 @@ def test_mixed_low_order_m2l_and_influence_match_f64(ctx):
     np.testing.assert_allclose(inf["mixed"], inf["f64"], rtol=1e-4, atol=0)
 
 
+@pytest.mark.parametrize("ls,p", [(5, 3), (6, 8)])
+def test_mixed_small_leaves_match_f64(ctx, ls, p):
+    # leaves of ~5 bodies run the warp-per-row packed near field and the grouped L2P on the
+    # mixed path: the result must agree with the FP64 solve to FP32 accuracy
+    buf = clustered(30000, 17)
+    outs = {}
+    for prec in ("f64", "mixed"):
+        og = fm.make_options(expansion_order=p, leaf_size_source=ls, multipole_acceptance=0.5,
+                             scalar_potential=True, precision=prec)
+        outs[prec], res = fm.solve_buffers(buf, L.FMM_POINT_SOURCE, og, ctx=ctx)
+        assert res.n_direct > 0 and res.n_m2l > 0
+    for rows in (slice(3, 4), slice(4, 7)):
+        assert rel_l2(outs["mixed"][:, rows], outs["f64"][:, rows]) < 1e-5
+
+
 def test_python_api_systems(ctx):
     rng = np.random.default_rng(5)
     n = 4000
