@@ -4,8 +4,11 @@
 // fmm_solve follows the reference driver (src/fmm.jl:807-1176): trees for the
 // targets and the sources, interaction lists, the influence estimate for the
 // relative error methods, then nearfield -> upward -> horizontal -> downward
-// passes and the unsort of the target buffer.  All stages run on one CUDA
-// stream; the tree and list builders synchronise with the host once per level.
+// passes and the unsort of the target buffer.  The trees, the lists, the near field
+// and the unsort run on the context's stream; the far field (upward pass, M2L,
+// downward pass) runs on a second high-priority stream concurrently with the near
+// field, and the influence estimate's sub-solve on a third; the tree and list
+// builders synchronise with the host once per level (trees) or per build (lists).
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -19,14 +22,19 @@ namespace {
 struct Workspace {
   DevTree tree[2];  // [0] target role, [1] source role (aliased when shared)
   DevLists lists;
-  DevBuf<double> acc13;  // target buffer rows 4..16, sorted order
+  DevBuf<double> acc13;      // target buffer rows 4..16, sorted order: near field (the whole field
+                             // when the far field runs on the same stream)
+  DevBuf<double> acc13_far;  // far field (L2P) when it runs on the far-field stream
   bool shared = false;
   DevTree& target() { return shared ? tree[1] : tree[0]; }
   DevTree& source() { return tree[1]; }
 };
 
+// far (may be null): the far field of the solve, added to the near field here with the
+// single addition the L2P makes when it accumulates into the near-field rows itself
 __global__ void k_unsort(const double* __restrict__ acc13, const int* __restrict__ sort_index,
-                         const double4* __restrict__ pos, int64_t n, double* __restrict__ out16) {
+                         const double4* __restrict__ pos, int64_t n, double* __restrict__ out16,
+                         const double* __restrict__ far = nullptr) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     int64_t o = sort_index ? sort_index[i] : i;
     double4 p = pos[i];
@@ -35,8 +43,14 @@ __global__ void k_unsort(const double* __restrict__ acc13, const int* __restrict
     d[1] = p.y;
     d[2] = p.z;
     const double* a = acc13 + 13 * i;
+    if (far) {
+      const double* f = far + 13 * i;
 #pragma unroll
-    for (int k = 0; k < 13; ++k) d[3 + k] = a[k];
+      for (int k = 0; k < 13; ++k) d[3 + k] = a[k] + f[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 13; ++k) d[3 + k] = a[k];
+    }
   }
 }
 
@@ -145,6 +159,9 @@ struct fmm_ctx {
   // influence estimate on its own stream (run_fmm)
   cudaStream_t est_stream = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // far field (upward, M2L, downward) on its own stream, concurrent with the near field
+  cudaStream_t far_stream = nullptr;
+  cudaEvent_t ev_far = nullptr;
   Scratch est_sc;
   DevBuf<int> est_stats;
   DevBuf<int> stats;
@@ -170,6 +187,18 @@ cudaEvent_t fork_event(fmm_ctx* c) {
 cudaEvent_t join_event(fmm_ctx* c) {
   if (!c->ev_join) FMM_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
   return c->ev_join;
+}
+cudaStream_t far_stream(fmm_ctx* c) {
+  if (!c->far_stream) {
+    int least = 0, greatest = 0;
+    FMM_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    FMM_CUDA_TRY(cudaStreamCreateWithPriority(&c->far_stream, cudaStreamNonBlocking, greatest));
+  }
+  return c->far_stream;
+}
+cudaEvent_t far_event(fmm_ctx* c) {
+  if (!c->ev_far) FMM_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_far, cudaEventDisableTiming));
+  return c->ev_far;
 }
 Scratch& est_scratch(fmm_ctx* c) { return c->est_sc; }
 DevBuf<int>& est_stats(fmm_ctx* c) { return c->est_stats; }
@@ -202,7 +231,7 @@ size_t footprint(const SolveIn& in, const fmm_options& o) {
   int64_t ls = std::max(1, o.leaf_size_source);
   int64_t nbr = 2 * (nt + in.n_s) / ls + 1024;
   size_t exp = (size_t)nbr * 4 * nh(o.expansion_order) * 8 * 2;
-  size_t bodies = (size_t)(nt + in.n_s) * (32 + 32 + 8) + (size_t)nt * (13 + 16) * 8;
+  size_t bodies = (size_t)(nt + in.n_s) * (32 + 32 + 8) + (size_t)nt * (13 + 13 + 16) * 8;
   size_t lists = (size_t)nbr * (256 + 64) * 8;
   size_t scratch = (size_t)(nt + in.n_s) * 48;
   return exp + bodies + lists + scratch;
@@ -213,13 +242,16 @@ size_t footprint(const SolveIn& in, const fmm_options& o) {
 cudaStream_t est_stream(fmm_ctx* c);
 cudaEvent_t fork_event(fmm_ctx* c);
 cudaEvent_t join_event(fmm_ctx* c);
+cudaStream_t far_stream(fmm_ctx* c);
+cudaEvent_t far_event(fmm_ctx* c);
 Scratch& est_scratch(fmm_ctx* c);
 DevBuf<int>& est_stats(fmm_ctx* c);
 
 // one fmm! evaluation into out16 (device, original target order), queued on st.
-// For the relative error methods the influence estimate (src/fmm.jl:1189-1276), which
-// only the M2L needs, runs on a second stream concurrently with the near field and the
-// upward pass; the M2L waits for it.
+// The far field runs on the far-field stream (M2L waiting for the influence estimate of
+// the relative error methods, src/fmm.jl:1189-1276, which runs on its own stream) while
+// the near field runs on st; st waits for the far field before the unsort.  The
+// estimate's own sub-solve keeps every stage on its stream.
 void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, double* out16, fmm_result* res,
              bool is_estimate, cudaStream_t st, Scratch& sc, DevBuf<int>& stats) {
   const int p = o.expansion_order;
@@ -261,8 +293,7 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   FMM_CUDA_TRY(cudaMemsetAsync(T.max_influence.ptr, 0, T.n_branches * sizeof(double), st));
   const bool estimate =
       o.error_method == FMM_POWER_RELATIVE_GRADIENT || o.error_method == FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT;
-  if (estimate) FMM_CUDA_TRY(cudaEventRecord(fork_event(c), st));
-  // ---- evaluation passes (src/fmm.jl:1028-1089): near field and upward pass
+  // ---- evaluation passes (src/fmm.jl:1028-1089)
   const int64_t NH4 = 4 * nh(p);
   upload_tables(c->tables, p, st);
   S.multipole.grow(NH4 * S.n_branches);
@@ -271,17 +302,41 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   FMM_CUDA_TRY(cudaMemsetAsync(T.local.ptr, 0, NH4 * T.n_branches * sizeof(double), st));
   W.acc13.grow(13 * (size_t)T.n_bodies);
   FMM_CUDA_TRY(cudaMemsetAsync(W.acc13.ptr, 0, 13 * T.n_bodies * sizeof(double), st));
+  // a solve runs its far field (upward pass, M2L, downward pass) on a second high-priority
+  // stream, concurrently with the near field on st, into its own accumulator; the influence
+  // estimate's sub-solve runs everything on its own stream
+  const bool split = !is_estimate;
+  double* far13 = W.acc13.ptr;
+  if (split) {
+    W.acc13_far.grow(13 * (size_t)T.n_bodies);
+    FMM_CUDA_TRY(cudaMemsetAsync(W.acc13_far.ptr, 0, 13 * T.n_bodies * sizeof(double), st));
+    far13 = W.acc13_far.ptr;
+  }
   stats.grow(8);
   FMM_CUDA_TRY(cudaMemsetAsync(stats.ptr, 0, 8 * sizeof(int), st));
   if (res) count_p2p_pairs(T, S, W.lists, reinterpret_cast<unsigned long long*>(stats.ptr + 4), st);
+  // bodies, trees, lists and zeroed accumulators are ready: fork the far field and the estimate
+  if (estimate || split) FMM_CUDA_TRY(cudaEventRecord(fork_event(c), st));
+  cudaStream_t fs = split ? far_stream(c) : st;
+  cudaEvent_t evf[5] = {};
+  if (timing && split)
+    for (auto& e : evf) FMM_CUDA_TRY(cudaEventCreate(&e));
+  auto markf = [&](int k) {
+    if (timing && split) FMM_CUDA_TRY(cudaEventRecord(evf[k], fs));
+  };
+  if (split) FMM_CUDA_TRY(cudaStreamWaitEvent(fs, fork_event(c), 0));
+  markf(0);
+  // near field
   launch_p2p(T, S, W.lists, W.acc13.ptr, in.kind, ps, gs, hs, o.precision, st);
   mark(3);
+  // upward pass
   if (o.upward_pass) {
-    launch_p2m(S, p, in.kind, c->tables, st);
-    launch_m2m(S, p, lh, c->tables, st);
+    launch_p2m(S, p, in.kind, c->tables, fs);
+    launch_m2m(S, p, lh, c->tables, fs);
   }
-  mark(4);
-  // ---- relative error methods: influence estimate on the second stream
+  markf(1);
+  if (!split) mark(4);
+  // ---- relative error methods: influence estimate on its own stream, joined before the M2L
   if (estimate) {
     fmm_options e = o;
     e.leaf_size_source = 5;
@@ -308,23 +363,31 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
     branch_max_influence(T, c->est_out16.ptr, es);
     if (timing) FMM_CUDA_TRY(cudaEventRecord(eve[1], es));
     FMM_CUDA_TRY(cudaEventRecord(join_event(c), es));
-    FMM_CUDA_TRY(cudaStreamWaitEvent(st, join_event(c), 0));
+    FMM_CUDA_TRY(cudaStreamWaitEvent(fs, join_event(c), 0));
   }
-  mark(5);
+  markf(2);
+  if (!split) mark(5);
   if (o.horizontal_pass)
     launch_m2l(T, S, W.lists, p, lh, o.error_method, o.error_tolerance, o.bonus_expansion, nullptr, stats.ptr,
-               c->tables, o.precision, st);
-  mark(6);
+               c->tables, o.precision, fs);
+  markf(3);
+  if (!split) mark(6);
   if (o.downward_pass) {
-    launch_l2l(T, p, lh, c->tables, st);
-    launch_l2p(T, p, lh, ps, gs, hs, W.acc13.ptr, st);
+    launch_l2l(T, p, lh, c->tables, fs);
+    launch_l2p(T, p, lh, ps, gs, hs, far13, fs);
+  }
+  markf(4);
+  if (split) {
+    FMM_CUDA_TRY(cudaEventRecord(far_event(c), fs));
+    FMM_CUDA_TRY(cudaStreamWaitEvent(st, far_event(c), 0));
   }
   // ---- unsort into the caller's order (buffer_to_target!, src/compatibility.jl:324-338)
   note_launch();
   if (is_estimate)  // out16 receives |grad| per body (n doubles)
     k_unsort_gradnorm<<<grid_for(T.n_bodies), 256, 0, st>>>(W.acc13.ptr, T.sort_index.ptr, T.n_bodies, out16);
   else
-    k_unsort<<<grid_for(T.n_bodies), 256, 0, st>>>(W.acc13.ptr, T.sort_index.ptr, T.pos.ptr, T.n_bodies, out16);
+    k_unsort<<<grid_for(T.n_bodies), 256, 0, st>>>(W.acc13.ptr, T.sort_index.ptr, T.pos.ptr, T.n_bodies, out16,
+                                                    split ? far13 : nullptr);
   FMM_CUDA_TRY(cudaGetLastError());
   mark(7);
   if (res) {
@@ -346,25 +409,31 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
     res->n_p2p_pairs = (int64_t)pairs;
     res->n_kernel_launches = g_launches - launches0;
     if (timing) {
-      float ms[7];
-      for (int k = 0; k < 7; ++k) FMM_CUDA_TRY(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
+      float ms[3], tot = 0.0f, fup = 0.0f, fh = 0.0f, fd = 0.0f;
+      for (int k = 0; k < 3; ++k) FMM_CUDA_TRY(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
+      FMM_CUDA_TRY(cudaEventElapsedTime(&tot, ev[0], ev[7]));
+      // far field on its own stream: upward (evf 0-1), horizontal (2-3, after the wait for the
+      // influence estimate), downward (3-4)
+      FMM_CUDA_TRY(cudaEventElapsedTime(&fup, evf[0], evf[1]));
+      FMM_CUDA_TRY(cudaEventElapsedTime(&fh, evf[2], evf[3]));
+      FMM_CUDA_TRY(cudaEventElapsedTime(&fd, evf[3], evf[4]));
       res->t_tree_ms = ms[0];
       res->t_lists_ms = ms[1];
       res->t_nearfield_ms = ms[2];
-      res->t_upward_ms = ms[3];
-      res->t_horizontal_ms = ms[5];  // ms[4]: waiting for the influence estimate
-      res->t_downward_ms = ms[6];
+      res->t_upward_ms = fup;
+      res->t_horizontal_ms = fh;
+      res->t_downward_ms = fd;
       float me = 0.0f;
       if (estimate) FMM_CUDA_TRY(cudaEventElapsedTime(&me, eve[0], eve[1]));
       res->t_influence_ms = me;  // on its own stream, overlapping the near field and the upward pass
-      float tot;
-      FMM_CUDA_TRY(cudaEventElapsedTime(&tot, ev[0], ev[7]));
       res->t_total_ms = tot;
     }
   }
   if (timing) {
     for (auto& e : ev) cudaEventDestroy(e);
     for (auto& e : eve) cudaEventDestroy(e);
+    for (auto& e : evf)
+      if (e) cudaEventDestroy(e);
   }
 }
 
@@ -484,6 +553,7 @@ int fmm_ctx_destroy(fmm_ctx* c) {
     release_tree(w->tree[1]);
     release_lists(w->lists);
     w->acc13.release();
+    w->acc13_far.release();
   }
   release_scratch(c->sc);
   release_scratch(c->est_sc);
@@ -492,6 +562,11 @@ int fmm_ctx_destroy(fmm_ctx* c) {
     cudaStreamSynchronize(c->est_stream);
     cudaStreamDestroy(c->est_stream);
   }
+  if (c->far_stream) {
+    cudaStreamSynchronize(c->far_stream);
+    cudaStreamDestroy(c->far_stream);
+  }
+  if (c->ev_far) cudaEventDestroy(c->ev_far);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
   c->tables.Hs.release();
@@ -535,7 +610,8 @@ size_t fmm_ctx_device_bytes(const fmm_ctx* c) {
   if (!c) return 0;
   size_t b = 0;
   for (const Workspace* w : {&c->main, &c->est}) {
-    b += tree_bytes(w->tree[0]) + tree_bytes(w->tree[1]) + lists_bytes(w->lists) + w->acc13.cap * 8;
+    b += tree_bytes(w->tree[0]) + tree_bytes(w->tree[1]) + lists_bytes(w->lists) +
+         (w->acc13.cap + w->acc13_far.cap) * 8;
   }
   const Scratch& s = c->sc;
   b += s.cub.cap + (s.keys_a.cap + s.keys_b.cap) * 8 +
