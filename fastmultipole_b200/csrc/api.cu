@@ -161,7 +161,7 @@ struct fmm_ctx {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // far field (upward, M2L, downward) on its own stream, concurrent with the near field
   cudaStream_t far_stream = nullptr;
-  cudaEvent_t ev_far = nullptr;
+  cudaEvent_t ev_far = nullptr, ev_up = nullptr;
   Scratch est_sc;
   DevBuf<int> est_stats;
   DevBuf<int> stats;
@@ -199,6 +199,10 @@ cudaStream_t far_stream(fmm_ctx* c) {
 cudaEvent_t far_event(fmm_ctx* c) {
   if (!c->ev_far) FMM_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_far, cudaEventDisableTiming));
   return c->ev_far;
+}
+cudaEvent_t up_event(fmm_ctx* c) {
+  if (!c->ev_up) FMM_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_up, cudaEventDisableTiming));
+  return c->ev_up;
 }
 Scratch& est_scratch(fmm_ctx* c) { return c->est_sc; }
 DevBuf<int>& est_stats(fmm_ctx* c) { return c->est_stats; }
@@ -244,6 +248,7 @@ cudaEvent_t fork_event(fmm_ctx* c);
 cudaEvent_t join_event(fmm_ctx* c);
 cudaStream_t far_stream(fmm_ctx* c);
 cudaEvent_t far_event(fmm_ctx* c);
+cudaEvent_t up_event(fmm_ctx* c);
 Scratch& est_scratch(fmm_ctx* c);
 DevBuf<int>& est_stats(fmm_ctx* c);
 
@@ -285,6 +290,32 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   }
   DevTree& T = W.target();
   mark(1);
+  // a solve runs its far field (upward pass, M2L, downward pass) on a second high-priority
+  // stream, concurrently with the lists and the near field on st, into its own accumulator;
+  // the influence estimate's sub-solve runs everything on its own stream
+  const bool split = !is_estimate;
+  cudaStream_t fs = split ? far_stream(c) : st;
+  cudaEvent_t evf[5] = {};
+  if (timing && split)
+    for (auto& e : evf) FMM_CUDA_TRY(cudaEventCreate(&e));
+  auto markf = [&](int k) {
+    if (timing && split) FMM_CUDA_TRY(cudaEventRecord(evf[k], fs));
+  };
+  const int64_t NH4 = 4 * nh(p);
+  upload_tables(c->tables, p, st);
+  S.multipole.grow(NH4 * S.n_branches);
+  FMM_CUDA_TRY(cudaMemsetAsync(S.multipole.ptr, 0, NH4 * S.n_branches * sizeof(double), st));
+  // ---- upward pass: needs the source tree only
+  if (split) {
+    FMM_CUDA_TRY(cudaEventRecord(up_event(c), st));
+    FMM_CUDA_TRY(cudaStreamWaitEvent(fs, up_event(c), 0));
+  }
+  markf(0);
+  if (o.upward_pass && split) {
+    launch_p2m(S, p, in.kind, c->tables, fs);
+    launch_m2m(S, p, lh, c->tables, fs);
+  }
+  markf(1);
   // ---- interaction lists (src/interaction_list.jl:3-19, 183-213)
   // error-controlled M2L: rows ordered by separation, so that the 32 pairs of a pass stop at similar orders
   build_lists(W.lists, T, S, sc, st, ls_s, o.multipole_acceptance, o.farfield != 0, o.nearfield != 0,
@@ -294,18 +325,10 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   const bool estimate =
       o.error_method == FMM_POWER_RELATIVE_GRADIENT || o.error_method == FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT;
   // ---- evaluation passes (src/fmm.jl:1028-1089)
-  const int64_t NH4 = 4 * nh(p);
-  upload_tables(c->tables, p, st);
-  S.multipole.grow(NH4 * S.n_branches);
   T.local.grow(NH4 * T.n_branches);
-  FMM_CUDA_TRY(cudaMemsetAsync(S.multipole.ptr, 0, NH4 * S.n_branches * sizeof(double), st));
   FMM_CUDA_TRY(cudaMemsetAsync(T.local.ptr, 0, NH4 * T.n_branches * sizeof(double), st));
   W.acc13.grow(13 * (size_t)T.n_bodies);
   FMM_CUDA_TRY(cudaMemsetAsync(W.acc13.ptr, 0, 13 * T.n_bodies * sizeof(double), st));
-  // a solve runs its far field (upward pass, M2L, downward pass) on a second high-priority
-  // stream, concurrently with the near field on st, into its own accumulator; the influence
-  // estimate's sub-solve runs everything on its own stream
-  const bool split = !is_estimate;
   double* far13 = W.acc13.ptr;
   if (split) {
     W.acc13_far.grow(13 * (size_t)T.n_bodies);
@@ -315,26 +338,16 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   stats.grow(8);
   FMM_CUDA_TRY(cudaMemsetAsync(stats.ptr, 0, 8 * sizeof(int), st));
   if (res) count_p2p_pairs(T, S, W.lists, reinterpret_cast<unsigned long long*>(stats.ptr + 4), st);
-  // bodies, trees, lists and zeroed accumulators are ready: fork the far field and the estimate
+  // trees, lists and zeroed accumulators are ready: fork the rest of the far field and the estimate
   if (estimate || split) FMM_CUDA_TRY(cudaEventRecord(fork_event(c), st));
-  cudaStream_t fs = split ? far_stream(c) : st;
-  cudaEvent_t evf[5] = {};
-  if (timing && split)
-    for (auto& e : evf) FMM_CUDA_TRY(cudaEventCreate(&e));
-  auto markf = [&](int k) {
-    if (timing && split) FMM_CUDA_TRY(cudaEventRecord(evf[k], fs));
-  };
   if (split) FMM_CUDA_TRY(cudaStreamWaitEvent(fs, fork_event(c), 0));
-  markf(0);
   // near field
   launch_p2p(T, S, W.lists, W.acc13.ptr, in.kind, ps, gs, hs, o.precision, st);
   mark(3);
-  // upward pass
-  if (o.upward_pass) {
-    launch_p2m(S, p, in.kind, c->tables, fs);
-    launch_m2m(S, p, lh, c->tables, fs);
+  if (o.upward_pass && !split) {
+    launch_p2m(S, p, in.kind, c->tables, st);
+    launch_m2m(S, p, lh, c->tables, st);
   }
-  markf(1);
   if (!split) mark(4);
   // ---- relative error methods: influence estimate on its own stream, joined before the M2L
   if (estimate) {
@@ -567,6 +580,7 @@ int fmm_ctx_destroy(fmm_ctx* c) {
     cudaStreamDestroy(c->far_stream);
   }
   if (c->ev_far) cudaEventDestroy(c->ev_far);
+  if (c->ev_up) cudaEventDestroy(c->ev_up);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
   c->tables.Hs.release();
