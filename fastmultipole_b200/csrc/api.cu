@@ -188,11 +188,14 @@ cudaEvent_t join_event(fmm_ctx* c) {
   if (!c->ev_join) FMM_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
   return c->ev_join;
 }
+// one priority level below the influence estimate's stream (when the device has one):
+// the M2L waits for the estimate, so the estimate's kernels go first
 cudaStream_t far_stream(fmm_ctx* c) {
   if (!c->far_stream) {
     int least = 0, greatest = 0;
     FMM_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    FMM_CUDA_TRY(cudaStreamCreateWithPriority(&c->far_stream, cudaStreamNonBlocking, greatest));
+    const int prio = greatest < least ? greatest + 1 : greatest;
+    FMM_CUDA_TRY(cudaStreamCreateWithPriority(&c->far_stream, cudaStreamNonBlocking, prio));
   }
   return c->far_stream;
 }
