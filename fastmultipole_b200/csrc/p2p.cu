@@ -159,8 +159,14 @@ struct Batch {
 // their batch holds per body {-x, -x, -y, -y}, {-z, -z, q, q} (ready-made pairs)
 template <class R, int KIND>
 __host__ __device__ constexpr bool packed() { return sizeof(R) == 4 && KIND == FMM_POINT_SOURCE; }
+// FP32 vortex particles: two targets per lane as well; batch per body {-x, -x, -y, -y},
+// {-z, -z, G0, G0}, {G1, G1, G2, G2}
 template <class R, int KIND>
-__host__ __device__ constexpr int slots_per_body() { return packed<R, KIND>() ? 8 : Batch<KIND>::nv; }
+__host__ __device__ constexpr bool packed_vortex() { return sizeof(R) == 4 && KIND == FMM_POINT_VORTEX; }
+template <class R, int KIND>
+__host__ __device__ constexpr int slots_per_body() {
+  return packed<R, KIND>() ? 8 : packed_vortex<R, KIND>() ? 12 : Batch<KIND>::nv;
+}
 // bodies per warp batch: the packed batch is halved to keep the same shared memory per CTA
 template <class R, int KIND>
 __host__ __device__ constexpr int batch_bodies() { return packed<R, KIND>() ? 128 : Batch<KIND>::n; }
@@ -253,6 +259,58 @@ __device__ __forceinline__ void packed_batch(const float4* __restrict__ B4, int 
   }
 }
 
+// One lane's slice of a packed vortex batch on its two targets: velocity
+// u = (G x d) / r^3 (GS) and its gradient (HS, the SMatrix column-major order of
+// test/vortex.jl:83-128), pairs with r^2 = 0 skipped.  acc[a] holds channel a of the
+// two targets.
+template <bool GS, bool HS, int NA>
+__device__ __forceinline__ void packed_vortex_batch(const float4* __restrict__ B4, int j0, int nb, int SS,
+                                                    float2 tx2, float2 ty2, float2 tz2, float2 (&acc)[NA]) {
+  constexpr int h = GS ? 3 : 0;
+  const float2 m1 = make_float2(-1.f, -1.f), m3 = make_float2(-3.f, -3.f);
+#pragma unroll 2
+  for (int j = j0; j < nb; j += SS) {
+    const float4 u = B4[3 * j], v = B4[3 * j + 1], w = B4[3 * j + 2];
+    const float2 dx = __fadd2_rn(tx2, make_float2(u.x, u.y));
+    const float2 dy = __fadd2_rn(ty2, make_float2(u.z, u.w));
+    const float2 dz = __fadd2_rn(tz2, make_float2(v.x, v.y));
+    const float2 g0 = make_float2(v.z, v.w), g1 = make_float2(w.x, w.y), g2 = make_float2(w.z, w.w);
+    float2 r2 = __fmul2_rn(dx, dx);
+    r2 = __ffma2_rn(dy, dy, r2);
+    r2 = __ffma2_rn(dz, dz, r2);
+    float2 ri;
+    ri.x = r2.x > 0.f ? rsqrt_ftz(r2.x) : 0.f;  // coincident bodies are skipped
+    ri.y = r2.y > 0.f ? rsqrt_ftz(r2.y) : 0.f;
+    const float2 ri2 = __fmul2_rn(ri, ri);
+    const float2 den = __fmul2_rn(ri, ri2);
+    // c = G x d
+    const float2 ng0 = __fmul2_rn(g0, m1), ng1 = __fmul2_rn(g1, m1), ng2 = __fmul2_rn(g2, m1);
+    const float2 cx = __ffma2_rn(g1, dz, __fmul2_rn(ng2, dy));
+    const float2 cy = __ffma2_rn(g2, dx, __fmul2_rn(ng0, dz));
+    const float2 cz = __ffma2_rn(g0, dy, __fmul2_rn(ng1, dx));
+    if (GS) {
+      acc[0] = __ffma2_rn(cx, den, acc[0]);
+      acc[1 % NA] = __ffma2_rn(cy, den, acc[1 % NA]);
+      acc[2 % NA] = __ffma2_rn(cz, den, acc[2 % NA]);
+    }
+    if (HS) {
+      const float2 d5 = __fmul2_rn(den, ri2);
+      const float2 m3d5 = __fmul2_rn(d5, m3);
+      const float2 px = __fmul2_rn(dx, m3d5), py = __fmul2_rn(dy, m3d5), pz = __fmul2_rn(dz, m3d5);
+      const float2 rd = __fmul2_rn(r2, d5);
+      acc[(h + 0) % NA] = __ffma2_rn(px, cx, acc[(h + 0) % NA]);
+      acc[(h + 1) % NA] = __ffma2_rn(px, cy, __ffma2_rn(g2, rd, acc[(h + 1) % NA]));
+      acc[(h + 2) % NA] = __ffma2_rn(px, cz, __ffma2_rn(ng1, rd, acc[(h + 2) % NA]));
+      acc[(h + 3) % NA] = __ffma2_rn(py, cx, __ffma2_rn(ng2, rd, acc[(h + 3) % NA]));
+      acc[(h + 4) % NA] = __ffma2_rn(py, cy, acc[(h + 4) % NA]);
+      acc[(h + 5) % NA] = __ffma2_rn(py, cz, __ffma2_rn(g0, rd, acc[(h + 5) % NA]));
+      acc[(h + 6) % NA] = __ffma2_rn(pz, cx, __ffma2_rn(g1, rd, acc[(h + 6) % NA]));
+      acc[(h + 7) % NA] = __ffma2_rn(pz, cy, __ffma2_rn(ng0, rd, acc[(h + 7) % NA]));
+      acc[(h + 8) % NA] = __ffma2_rn(pz, cz, acc[(h + 8) % NA]);
+    }
+  }
+}
+
 // RW: one warp per row (rows of small leaves, kWarps rows per CTA), the warp adding its
 // sums to the targets itself; otherwise one CTA per row, the warps splitting its sources.
 template <class R, int KIND, bool PS, bool GS, bool HS, bool RW>
@@ -267,7 +325,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
   constexpr int NS = slots_per_body<R, KIND>();
   constexpr bool MIXED = sizeof(R) == 4;
   constexpr bool PACK = packed<R, KIND>();
-  static_assert(!PACK || kTPT == 2, "packed path pairs two targets per lane");
+  constexpr bool PACKV = packed_vortex<R, KIND>();
+  static_assert((!PACK && !PACKV) || kTPT == 2, "packed paths pair two targets per lane");
   extern __shared__ __align__(16) unsigned char p2p_smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   R* B = reinterpret_cast<R*>(p2p_smem) + w * NS * NB;  // this warp's batch, plane v at B[v * NB]
@@ -357,6 +416,16 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
           float4* B4 = reinterpret_cast<float4*>(B);
           B4[2 * idx] = make_float4(x, x, y, y);
           B4[2 * idx + 1] = make_float4(z, z, q, q);
+        } else if (PACKV && idx < nb) {
+          const int body = sk + idx - ek;
+          const double4 p = spos[body];
+          const double4 g = sstr[body];
+          const float x = -(float)(p.x - ox), y = -(float)(p.y - oy), z = -(float)(p.z - oz);
+          const float g0 = (float)g.x, g1 = (float)g.y, g2 = (float)g.z;
+          float4* B4 = reinterpret_cast<float4*>(B);
+          B4[3 * idx] = make_float4(x, x, y, y);
+          B4[3 * idx + 1] = make_float4(z, z, g0, g0);
+          B4[3 * idx + 2] = make_float4(g1, g1, g2, g2);
         } else if (idx < nb) {
           const int body = sk + idx - ek;
           double4 p = spos[body];
@@ -399,6 +468,19 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
         part[1][2 % NA] += (R)gy.y;
         part[0][3 % NA] += (R)gz.x;
         part[1][3 % NA] += (R)gz.y;
+      } else if constexpr (PACKV) {
+        const float2 tx2 = make_float2((float)tx[0], (float)tx[1]);
+        const float2 ty2 = make_float2((float)ty[0], (float)ty[1]);
+        const float2 tz2 = make_float2((float)tz[0], (float)tz[1]);
+        float2 acc[NA];
+#pragma unroll
+        for (int a = 0; a < NA; ++a) acc[a] = make_float2(0.f, 0.f);
+        packed_vortex_batch<GS, HS, NA>(reinterpret_cast<const float4*>(B), slice, nb, SS, tx2, ty2, tz2, acc);
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+          part[0][a] += (R)acc[a].x;
+          part[1][a] += (R)acc[a].y;
+        }
       } else {
         for (int j = slice; j < nb; j += SS) {
           const R sx = B[j], sy = B[NB + j], sz = B[2 * NB + j], s0 = B[3 * NB + j];
