@@ -172,6 +172,21 @@ def test_mixed_vortex_matches_f64(ctx):
             assert rel_l2(omx[:, rows], o64[:, rows]) < 1e-5
 
 
+@pytest.mark.parametrize("p", [4, 12])
+def test_mixed_vortex_far_field_matches_f64(ctx, p):
+    # far field only: the mixed path's lane-per-pair Lamb-Helmholtz M2L (FP32 rotations of
+    # scaled multipoles) against the FP64 engine, velocity and velocity gradient
+    buf = ring(30000, 9)
+    outs = {}
+    for prec in ("f64", "mixed"):
+        og = fm.make_options(expansion_order=p, leaf_size_source=40, multipole_acceptance=0.4, nearfield=False,
+                             hessian=True, precision=prec)
+        outs[prec], res = fm.solve_buffers(buf, L.FMM_POINT_VORTEX, og, ctx=ctx)
+        assert res.n_m2l > 0
+    for rows in (slice(4, 7), slice(7, 16)):
+        assert rel_l2(outs["mixed"][:, rows], outs["f64"][:, rows]) < 1e-5
+
+
 @pytest.mark.parametrize("em", [fm.PowerRelativeGradient(1e-6), fm.PowerAbsoluteGradient(1e-4),
                                 fm.RotatedCoefficientsRelativeGradient(1e-6)], ids=["prg", "pag", "rcrg"])
 def test_error_controlled_orders_match_oracle(ctx, em):
