@@ -1222,35 +1222,37 @@ struct L2LLaneGo {
   void go() { run_l2l_lane<P>(t, st); }
 };
 
-// ---- Lamb-Helmholtz (vortex particle) plain M2L, mixed precision -------------------
+// ---- Lamb-Helmholtz (vortex particle) plain M2L ---------------------------------
 // One warp per target branch, one lane per (target, source) pair, as k_m2l_lane.  The two
-// expansion sets (phi: 0, chi: 1) share every rotation.  Before the FP32 rotations set 0 of
+// expansion sets (phi: 0, chi: 1) share every rotation.  Before the rotations (in V: FP32 on the
+// mixed path, FP64 on the drop-in path) set 0 of
 // the multipole is scaled by t^-n and set 1 by t^(1-n); the coaxial translation with (n+n')!
 // then gives the local sets times t^(n+1) and t^(n+2), on which the Lamb-Helmholtz coupling
 // of transform_lamb_helmholtz_local! (src/translate.jl:98-142) needs no power of t:
 //   phi(n, m) -= i (m / n) chi(n, m),  chi(n, m) -= chi(n + 1, m) / (n + 1).
 // The rotated-back degrees are scaled by t^-(n+1) / t^-(n+2) in FP64 and summed over the
 // lanes through shared memory into the warp's FP64 accumulator.
-__device__ __forceinline__ float& MSl(float* Ms, int i, int c, int lane) { return Ms[(4 * i + c) * 32 + lane]; }
+template <class V>
+__device__ __forceinline__ V& MSl(V* Ms, int i, int c, int lane) { return Ms[(4 * i + c) * 32 + lane]; }
 
-template <int PMAX>
+template <int PMAX, class V>
 constexpr size_t lane_lh_smem_bytes() {
   return ((size_t)4 * (PMAX + 1) * 33 + (size_t)4 * hi(PMAX + 1, 0)) * sizeof(double) +
-         (size_t)4 * hi(PMAX + 1, 0) * 32 * sizeof(float);
+         (size_t)4 * hi(PMAX + 1, 0) * 32 * sizeof(V);
 }
 
 // coaxial translation of one set (c0 = 0 or 2) of degree n, scaled: sum_{n'} (n+n')! M(n', m)
-template <int PMAX>
-__device__ __forceinline__ void coax_lh(int n, int P, const float* Ms, int c0, int lane, float (&Xr)[PMAX + 1],
-                                        float (&Xi)[PMAX + 1]) {
+template <int PMAX, class V>
+__device__ __forceinline__ void coax_lh(int n, int P, const V* Ms, int c0, int lane, V (&Xr)[PMAX + 1],
+                                        V (&Xi)[PMAX + 1]) {
 #pragma unroll
   for (int m = 0; m <= PMAX; ++m) {
-    Xr[m] = Xi[m] = 0.0f;
+    Xr[m] = Xi[m] = V(0);
     if (m > n) continue;
-    float vr = 0.f, vi = 0.f;
+    V vr = 0, vi = 0;
 #pragma unroll 1
     for (int np = m; np <= P; ++np) {
-      const float c = c_factF[n + np];
+      const V c = sizeof(V) == 4 ? (V)c_factF[n + np] : (V)c_fact[n + np];
       vr += c * Ms[(4 * hi(np, m) + c0) * 32 + lane];
       vi += c * Ms[(4 * hi(np, m) + c0 + 1) * 32 + lane];
     }
@@ -1259,7 +1261,7 @@ __device__ __forceinline__ void coax_lh(int n, int P, const float* Ms, int c0, i
   }
 }
 
-template <int PMAX>
+template <int PMAX, class V>
 __global__ void __launch_bounds__(32) k_m2l_lane_lh(const int* __restrict__ tgt_list, const int* __restrict__ off,
                                                     const int* __restrict__ src_of, double* __restrict__ local,
                                                     const double* __restrict__ multipole,
@@ -1270,7 +1272,7 @@ __global__ void __launch_bounds__(32) k_m2l_lane_lh(const int* __restrict__ tgt_
   extern __shared__ double lane_smem[];
   double* stage = lane_smem;                   // [4 (PMAX+1)][33]
   double* acc = stage + 4 * (PMAX + 1) * 33;   // [4 NH]
-  float* Ms = reinterpret_cast<float*>(acc + 4 * NH);  // rotated multipole [4 NH][32]
+  V* Ms = reinterpret_cast<V*>(acc + 4 * NH);  // rotated multipole [4 NH][32]
   const int lane = threadIdx.x;
   const int b = blockIdx.x;
   const int t = tgt_list[b];
@@ -1300,39 +1302,39 @@ __global__ void __launch_bounds__(32) k_m2l_lane_lh(const int* __restrict__ tgt_
       rinv = 1 / r;
       if (p_used) p_used[l] = P;
     }
-    const float fcph = (float)cph, fsph = (float)sph, fcth = (float)cth, fsth = (float)sth;
+    const V fcph = (V)cph, fsph = (V)sph, fcth = (V)cth, fsth = (V)sth;
     // forward: both sets of every degree, rotated, scaled (t^-n and t^(1-n))
     double sc = 1.0;  // t^-n
 #pragma unroll 1
     for (int n = 0; n <= P; ++n) {
       if (n > 0) sc *= rinv;
       const double sc1 = sc / rinv;  // t^(1-n)
-      float X0r[PMAX + 1], X0i[PMAX + 1], X1r[PMAX + 1], X1i[PMAX + 1];
+      V X0r[PMAX + 1], X0i[PMAX + 1], X1r[PMAX + 1], X1i[PMAX + 1];
       double er = 1.0, ei = 0.0;
       const int base = hi(n, 0);
 #pragma unroll
       for (int a = 0; a <= PMAX; ++a) {
-        X0r[a] = X0i[a] = X1r[a] = X1i[a] = 0.0f;
+        X0r[a] = X0i[a] = X1r[a] = X1i[a] = V(0);
         if (a > n || !valid) continue;
         const double2 u = __ldg(reinterpret_cast<const double2*>(src) + 2 * (base + a));
         const double2 v = __ldg(reinterpret_cast<const double2*>(src) + 2 * (base + a) + 1);
-        X0r[a] = (float)((u.x * er - u.y * ei) * sc);
-        X0i[a] = (float)((u.x * ei + u.y * er) * sc);
-        X1r[a] = (float)((v.x * er - v.y * ei) * sc1);
-        X1i[a] = (float)((v.x * ei + v.y * er) * sc1);
+        X0r[a] = (V)((u.x * er - u.y * ei) * sc);
+        X0i[a] = (V)((u.x * ei + u.y * er) * sc);
+        X1r[a] = (V)((v.x * er - v.y * ei) * sc1);
+        X1i[a] = (V)((v.x * ei + v.y * er) * sc1);
         const double tt = er;
         er = er * cph - ei * sph;
         ei = tt * sph + ei * cph;
       }
-      float Yr[PMAX + 1], Yi[PMAX + 1];
-      rot_y<PMAX, false, float>(n, X0r, X0i, fcth, fsth, Yr, Yi);
+      V Yr[PMAX + 1], Yi[PMAX + 1];
+      rot_y<PMAX, false, V>(n, X0r, X0i, fcth, fsth, Yr, Yi);
 #pragma unroll
       for (int m = 0; m <= PMAX; ++m) {
         if (m > n) break;
         MSl(Ms, base + m, 0, lane) = Yr[m];
         MSl(Ms, base + m, 1, lane) = Yi[m];
       }
-      rot_y<PMAX, false, float>(n, X1r, X1i, fcth, fsth, Yr, Yi);
+      rot_y<PMAX, false, V>(n, X1r, X1i, fcth, fsth, Yr, Yi);
 #pragma unroll
       for (int m = 0; m <= PMAX; ++m) {
         if (m > n) break;
@@ -1343,74 +1345,75 @@ __global__ void __launch_bounds__(32) k_m2l_lane_lh(const int* __restrict__ tgt_
     __syncwarp();
     // back: per degree the coaxial translation of set 0 (degree n) and of set 1 one degree
     // ahead, the Lamb-Helmholtz coupling, both sets rotated back, scaled and staged
-    float C1r[PMAX + 1], C1i[PMAX + 1];  // set 1 of degree n before the coupling
-    coax_lh<PMAX>(0, P, Ms, 2, lane, C1r, C1i);
+    V C1r[PMAX + 1], C1i[PMAX + 1];  // set 1 of degree n before the coupling
+    coax_lh<PMAX, V>(0, P, Ms, 2, lane, C1r, C1i);
     double tn1 = rinv;  // t^-(n+1)
 #pragma unroll 1
     for (int n = 0; n <= P; ++n) {
       if (n > 0) tn1 *= rinv;
       const double tn2 = tn1 * rinv;
-      float N1r[PMAX + 1], N1i[PMAX + 1];  // set 1 of degree n + 1 before the coupling
+      V N1r[PMAX + 1], N1i[PMAX + 1];  // set 1 of degree n + 1 before the coupling
       if (n < P) {
-        coax_lh<PMAX>(n + 1, P, Ms, 2, lane, N1r, N1i);
+        coax_lh<PMAX, V>(n + 1, P, Ms, 2, lane, N1r, N1i);
       } else {
 #pragma unroll
-        for (int m = 0; m <= PMAX; ++m) N1r[m] = N1i[m] = 0.0f;
+        for (int m = 0; m <= PMAX; ++m) N1r[m] = N1i[m] = V(0);
       }
-      float Xr[PMAX + 1], Xi[PMAX + 1], Yr[PMAX + 1], Yi[PMAX + 1];
+      V Xr[PMAX + 1], Xi[PMAX + 1], Yr[PMAX + 1], Yi[PMAX + 1];
       // set 0: phi(n, m) - i (m / n) chi(n, m)
-      coax_lh<PMAX>(n, P, Ms, 0, lane, Xr, Xi);
+      coax_lh<PMAX, V>(n, P, Ms, 0, lane, Xr, Xi);
       if (n > 0) {
-        const float inv_n = 1.0f / (float)n;
+        const V inv_n = V(1) / (V)n;
 #pragma unroll
         for (int m = 0; m <= PMAX; ++m) {
           if (m > n) break;
-          const float a = (float)m * inv_n;
+          const V a = (V)m * inv_n;
           Xr[m] -= a * C1i[m];
           Xi[m] += a * C1r[m];
         }
       }
-      rot_y<PMAX, true, float>(n, Xr, Xi, fcth, fsth, Yr, Yi);
-      float er = 1.0f, ei = 0.0f;
+      rot_y<PMAX, true, V>(n, Xr, Xi, fcth, fsth, Yr, Yi);
+      V er = 1, ei = 0;
 #pragma unroll
       for (int m = 0; m <= PMAX; ++m) {
         if (m > n) break;
-        const float vr = Yr[m] * er + Yi[m] * ei;  // times e^{-i m phi}
-        const float vi = Yi[m] * er - Yr[m] * ei;
+        const V vr = Yr[m] * er + Yi[m] * ei;  // times e^{-i m phi}
+        const V vi = Yi[m] * er - Yr[m] * ei;
         stage[(4 * m) * 33 + lane] = valid ? vr * tn1 : 0.0;
         stage[(4 * m + 1) * 33 + lane] = valid ? vi * tn1 : 0.0;
-        const float tt = er;
+        const V tt = er;
         er = er * fcph - ei * fsph;
         ei = tt * fsph + ei * fcph;
       }
       // set 1: chi(n, m) - chi(n + 1, m) / (n + 1)
-      const float inv_n1 = 1.0f / (float)(n + 1);
+      const V inv_n1 = V(1) / (V)(n + 1);
 #pragma unroll
       for (int m = 0; m <= PMAX; ++m) {
         Xr[m] = C1r[m] - inv_n1 * N1r[m];
         Xi[m] = C1i[m] - inv_n1 * N1i[m];
-        if (m > n) Xr[m] = Xi[m] = 0.0f;
+        if (m > n) Xr[m] = Xi[m] = V(0);
       }
-      rot_y<PMAX, true, float>(n, Xr, Xi, fcth, fsth, Yr, Yi);
-      er = 1.0f;
-      ei = 0.0f;
+      rot_y<PMAX, true, V>(n, Xr, Xi, fcth, fsth, Yr, Yi);
+      er = 1;
+      ei = 0;
 #pragma unroll
       for (int m = 0; m <= PMAX; ++m) {
         if (m > n) break;
-        const float vr = Yr[m] * er + Yi[m] * ei;
-        const float vi = Yi[m] * er - Yr[m] * ei;
+        const V vr = Yr[m] * er + Yi[m] * ei;
+        const V vi = Yi[m] * er - Yr[m] * ei;
         stage[(4 * m + 2) * 33 + lane] = valid ? vr * tn2 : 0.0;
         stage[(4 * m + 3) * 33 + lane] = valid ? vi * tn2 : 0.0;
-        const float tt = er;
+        const V tt = er;
         er = er * fcph - ei * fsph;
         ei = tt * fsph + ei * fcph;
       }
       __syncwarp();
-      if (lane < 4 * (n + 1)) {
+      // 4 (n + 1) staged rows: more than the warp's 32 lanes from degree 8
+      for (int row = lane; row < 4 * (n + 1); row += 32) {
         double v = 0.0;
 #pragma unroll 8
-        for (int k = 0; k < 32; ++k) v += stage[lane * 33 + k];
-        acc[4 * hi(n, 0) + lane] += v;
+        for (int k = 0; k < 32; ++k) v += stage[row * 33 + k];
+        acc[4 * hi(n, 0) + row] += v;
       }
       __syncwarp();
 #pragma unroll
@@ -1429,17 +1432,25 @@ __global__ void __launch_bounds__(32) k_m2l_lane_lh(const int* __restrict__ tgt_
   }
 }
 
-template <int PMAX>
-void run_m2l_lane_lh(DevTree& t, const DevTree& s, const DevLists& L, int P, int* p_used, int* stats,
-                     cudaStream_t st) {
-  constexpr size_t sm = lane_lh_smem_bytes<PMAX>();
+template <int PMAX, class V>
+void run_m2l_lane_lh_v(DevTree& t, const DevTree& s, const DevLists& L, int P, int* p_used, int* stats,
+                       cudaStream_t st) {
+  constexpr size_t sm = lane_lh_smem_bytes<PMAX, V>();
   if (sm > 48 * 1024)
-    FMM_CUDA_TRY(cudaFuncSetAttribute(k_m2l_lane_lh<PMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    FMM_CUDA_TRY(cudaFuncSetAttribute(k_m2l_lane_lh<PMAX, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   note_launch();
-  k_m2l_lane_lh<PMAX><<<(int)L.n_m2l_targets, 32, sm, st>>>(
+  k_m2l_lane_lh<PMAX, V><<<(int)L.n_m2l_targets, 32, sm, st>>>(
       L.m2l_tgt.ptr, L.m2l_off.ptr, L.m2l_s.ptr, t.local.ptr, s.multipole.ptr, t.tcenter.ptr, s.scenter.ptr, P,
       p_used, stats, reinterpret_cast<unsigned long long*>(stats + 2));
   FMM_CUDA_TRY(cudaGetLastError());
+}
+template <int PMAX>
+void run_m2l_lane_lh(DevTree& t, const DevTree& s, const DevLists& L, int P, int* p_used, int* stats, int precision,
+                     cudaStream_t st) {
+  if (precision == FMM_PRECISION_MIXED)
+    run_m2l_lane_lh_v<PMAX, float>(t, s, L, P, p_used, stats, st);
+  else
+    run_m2l_lane_lh_v<PMAX, double>(t, s, L, P, p_used, stats, st);
 }
 
 }  // namespace
@@ -1448,21 +1459,21 @@ bool launch_m2l_lane(DevTree& t, const DevTree& s, const DevLists& L, int p, boo
                      int* p_used, int* stats, int precision, cudaStream_t st) {
   if (p < 1 || p > kLaneMaxP) return false;
   if (lh) {
-    // vortex particles: the plain mixed-precision M2L from order 4 (orders <= 3 take the
-    // thread-per-pair kernel, the FP64 and error-controlled ones the general engine)
-    if (em != FMM_ERROR_NONE || precision != FMM_PRECISION_MIXED || p < 4) return false;
+    // vortex particles: the plain M2L from order 4 (orders <= 3 take the thread-per-pair
+    // kernel, the error-controlled ones the general engine)
+    if (em != FMM_ERROR_NONE || p < 4) return false;
     if (L.n_m2l_targets == 0) return true;
     ensure_lane_tables(st);
     switch (p) {
-      case 4: run_m2l_lane_lh<4>(t, s, L, p, p_used, stats, st); break;
-      case 5: run_m2l_lane_lh<5>(t, s, L, p, p_used, stats, st); break;
-      case 6: run_m2l_lane_lh<6>(t, s, L, p, p_used, stats, st); break;
-      case 7: run_m2l_lane_lh<7>(t, s, L, p, p_used, stats, st); break;
-      case 8: run_m2l_lane_lh<8>(t, s, L, p, p_used, stats, st); break;
-      case 9: run_m2l_lane_lh<9>(t, s, L, p, p_used, stats, st); break;
-      case 10: run_m2l_lane_lh<10>(t, s, L, p, p_used, stats, st); break;
-      case 11: run_m2l_lane_lh<11>(t, s, L, p, p_used, stats, st); break;
-      default: run_m2l_lane_lh<12>(t, s, L, p, p_used, stats, st); break;
+      case 4: run_m2l_lane_lh<4>(t, s, L, p, p_used, stats, precision, st); break;
+      case 5: run_m2l_lane_lh<5>(t, s, L, p, p_used, stats, precision, st); break;
+      case 6: run_m2l_lane_lh<6>(t, s, L, p, p_used, stats, precision, st); break;
+      case 7: run_m2l_lane_lh<7>(t, s, L, p, p_used, stats, precision, st); break;
+      case 8: run_m2l_lane_lh<8>(t, s, L, p, p_used, stats, precision, st); break;
+      case 9: run_m2l_lane_lh<9>(t, s, L, p, p_used, stats, precision, st); break;
+      case 10: run_m2l_lane_lh<10>(t, s, L, p, p_used, stats, precision, st); break;
+      case 11: run_m2l_lane_lh<11>(t, s, L, p, p_used, stats, precision, st); break;
+      default: run_m2l_lane_lh<12>(t, s, L, p, p_used, stats, precision, st); break;
     }
     return true;
   }
