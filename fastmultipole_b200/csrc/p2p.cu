@@ -259,55 +259,86 @@ __device__ __forceinline__ void packed_batch(const float4* __restrict__ B4, int 
   }
 }
 
+// f32x2 with both halves negated
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
 // One lane's slice of a packed vortex batch on its two targets: velocity
 // u = (G x d) / r^3 (GS) and its gradient (HS, the SMatrix column-major order of
-// test/vortex.jl:83-128), pairs with r^2 = 0 skipped.  acc[a] holds channel a of the
-// two targets.
-template <bool GS, bool HS, int NA>
+// test/vortex.jl:83-128).  acc[a] receives channel a of the two targets.  The gradient
+// du_j/dx_i = eps_jki G_k / r^3 - 3 d_i (G x d)_j / r^5 is summed as two parts, Q_ij =
+// sum d_i (G x d)_j / r^5 and E_k = sum G_k / r^3, combined once per batch (r^2 / r^5 =
+// 1 / r^3, so the six eps terms need three sums).  GUARD skips pairs with r^2 = 0
+// (coincident bodies); without it such a pair makes the sums non-finite.
+template <bool GUARD, bool GS, bool HS, int NA>
 __device__ __forceinline__ void packed_vortex_batch(const float4* __restrict__ B4, int j0, int nb, int SS,
                                                     float2 tx2, float2 ty2, float2 tz2, float2 (&acc)[NA]) {
   constexpr int h = GS ? 3 : 0;
-  const float2 m1 = make_float2(-1.f, -1.f), m3 = make_float2(-3.f, -3.f);
+  float2 u[3], Q[9], E[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) u[a] = E[a] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int a = 0; a < 9; ++a) Q[a] = make_float2(0.f, 0.f);
 #pragma unroll 2
   for (int j = j0; j < nb; j += SS) {
-    const float4 u = B4[3 * j], v = B4[3 * j + 1], w = B4[3 * j + 2];
-    const float2 dx = __fadd2_rn(tx2, make_float2(u.x, u.y));
-    const float2 dy = __fadd2_rn(ty2, make_float2(u.z, u.w));
+    const float4 p = B4[3 * j], v = B4[3 * j + 1], w = B4[3 * j + 2];
+    const float2 dx = __fadd2_rn(tx2, make_float2(p.x, p.y));
+    const float2 dy = __fadd2_rn(ty2, make_float2(p.z, p.w));
     const float2 dz = __fadd2_rn(tz2, make_float2(v.x, v.y));
     const float2 g0 = make_float2(v.z, v.w), g1 = make_float2(w.x, w.y), g2 = make_float2(w.z, w.w);
     float2 r2 = __fmul2_rn(dx, dx);
     r2 = __ffma2_rn(dy, dy, r2);
     r2 = __ffma2_rn(dz, dz, r2);
     float2 ri;
-    ri.x = r2.x > 0.f ? rsqrt_ftz(r2.x) : 0.f;  // coincident bodies are skipped
-    ri.y = r2.y > 0.f ? rsqrt_ftz(r2.y) : 0.f;
+    if (GUARD) {
+      ri.x = r2.x > 0.f ? rsqrt_ftz(r2.x) : 0.f;
+      ri.y = r2.y > 0.f ? rsqrt_ftz(r2.y) : 0.f;
+    } else {
+      ri = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+    }
     const float2 ri2 = __fmul2_rn(ri, ri);
     const float2 den = __fmul2_rn(ri, ri2);
     // c = G x d
-    const float2 ng0 = __fmul2_rn(g0, m1), ng1 = __fmul2_rn(g1, m1), ng2 = __fmul2_rn(g2, m1);
-    const float2 cx = __ffma2_rn(g1, dz, __fmul2_rn(ng2, dy));
-    const float2 cy = __ffma2_rn(g2, dx, __fmul2_rn(ng0, dz));
-    const float2 cz = __ffma2_rn(g0, dy, __fmul2_rn(ng1, dx));
+    const float2 cx = __ffma2_rn(g1, dz, neg2(__fmul2_rn(g2, dy)));
+    const float2 cy = __ffma2_rn(g2, dx, neg2(__fmul2_rn(g0, dz)));
+    const float2 cz = __ffma2_rn(g0, dy, neg2(__fmul2_rn(g1, dx)));
     if (GS) {
-      acc[0] = __ffma2_rn(cx, den, acc[0]);
-      acc[1 % NA] = __ffma2_rn(cy, den, acc[1 % NA]);
-      acc[2 % NA] = __ffma2_rn(cz, den, acc[2 % NA]);
+      u[0] = __ffma2_rn(cx, den, u[0]);
+      u[1] = __ffma2_rn(cy, den, u[1]);
+      u[2] = __ffma2_rn(cz, den, u[2]);
     }
     if (HS) {
       const float2 d5 = __fmul2_rn(den, ri2);
-      const float2 m3d5 = __fmul2_rn(d5, m3);
-      const float2 px = __fmul2_rn(dx, m3d5), py = __fmul2_rn(dy, m3d5), pz = __fmul2_rn(dz, m3d5);
-      const float2 rd = __fmul2_rn(r2, d5);
-      acc[(h + 0) % NA] = __ffma2_rn(px, cx, acc[(h + 0) % NA]);
-      acc[(h + 1) % NA] = __ffma2_rn(px, cy, __ffma2_rn(g2, rd, acc[(h + 1) % NA]));
-      acc[(h + 2) % NA] = __ffma2_rn(px, cz, __ffma2_rn(ng1, rd, acc[(h + 2) % NA]));
-      acc[(h + 3) % NA] = __ffma2_rn(py, cx, __ffma2_rn(ng2, rd, acc[(h + 3) % NA]));
-      acc[(h + 4) % NA] = __ffma2_rn(py, cy, acc[(h + 4) % NA]);
-      acc[(h + 5) % NA] = __ffma2_rn(py, cz, __ffma2_rn(g0, rd, acc[(h + 5) % NA]));
-      acc[(h + 6) % NA] = __ffma2_rn(pz, cx, __ffma2_rn(g1, rd, acc[(h + 6) % NA]));
-      acc[(h + 7) % NA] = __ffma2_rn(pz, cy, __ffma2_rn(ng0, rd, acc[(h + 7) % NA]));
-      acc[(h + 8) % NA] = __ffma2_rn(pz, cz, acc[(h + 8) % NA]);
+      const float2 px = __fmul2_rn(dx, d5), py = __fmul2_rn(dy, d5), pz = __fmul2_rn(dz, d5);
+      Q[0] = __ffma2_rn(px, cx, Q[0]);
+      Q[1] = __ffma2_rn(px, cy, Q[1]);
+      Q[2] = __ffma2_rn(px, cz, Q[2]);
+      Q[3] = __ffma2_rn(py, cx, Q[3]);
+      Q[4] = __ffma2_rn(py, cy, Q[4]);
+      Q[5] = __ffma2_rn(py, cz, Q[5]);
+      Q[6] = __ffma2_rn(pz, cx, Q[6]);
+      Q[7] = __ffma2_rn(pz, cy, Q[7]);
+      Q[8] = __ffma2_rn(pz, cz, Q[8]);
+      E[0] = __ffma2_rn(g0, den, E[0]);
+      E[1] = __ffma2_rn(g1, den, E[1]);
+      E[2] = __ffma2_rn(g2, den, E[2]);
     }
+  }
+  if (GS) {
+    acc[0] = u[0];
+    acc[1 % NA] = u[1];
+    acc[2 % NA] = u[2];
+  }
+  if (HS) {
+    const float2 m3 = make_float2(-3.f, -3.f);
+    acc[(h + 0) % NA] = __fmul2_rn(m3, Q[0]);
+    acc[(h + 1) % NA] = __ffma2_rn(m3, Q[1], E[2]);
+    acc[(h + 2) % NA] = __ffma2_rn(m3, Q[2], neg2(E[1]));
+    acc[(h + 3) % NA] = __ffma2_rn(m3, Q[3], neg2(E[2]));
+    acc[(h + 4) % NA] = __fmul2_rn(m3, Q[4]);
+    acc[(h + 5) % NA] = __ffma2_rn(m3, Q[5], E[0]);
+    acc[(h + 6) % NA] = __ffma2_rn(m3, Q[6], E[1]);
+    acc[(h + 7) % NA] = __ffma2_rn(m3, Q[7], neg2(E[0]));
+    acc[(h + 8) % NA] = __fmul2_rn(m3, Q[8]);
   }
 }
 
@@ -472,10 +503,18 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
         const float2 tx2 = make_float2((float)tx[0], (float)tx[1]);
         const float2 ty2 = make_float2((float)ty[0], (float)ty[1]);
         const float2 tz2 = make_float2((float)tz[0], (float)tz[1]);
+        const float4* B4 = reinterpret_cast<const float4*>(B);
         float2 acc[NA];
+        // as on the point-source path: only batches holding the target's own leaf guard every pair
+        if (self_batch) {
+          packed_vortex_batch<true, GS, HS, NA>(B4, slice, nb, SS, tx2, ty2, tz2, acc);
+        } else {
+          packed_vortex_batch<false, GS, HS, NA>(B4, slice, nb, SS, tx2, ty2, tz2, acc);
+          float sum = 0.f;
 #pragma unroll
-        for (int a = 0; a < NA; ++a) acc[a] = make_float2(0.f, 0.f);
-        packed_vortex_batch<GS, HS, NA>(reinterpret_cast<const float4*>(B), slice, nb, SS, tx2, ty2, tz2, acc);
+          for (int a = 0; a < NA; ++a) sum += acc[a].x + acc[a].y;
+          if (!isfinite(sum)) packed_vortex_batch<true, GS, HS, NA>(B4, slice, nb, SS, tx2, ty2, tz2, acc);
+        }
 #pragma unroll
         for (int a = 0; a < NA; ++a) {
           part[0][a] += (R)acc[a].x;

@@ -109,6 +109,10 @@ CASES = [
                  interaction_list_method=fm.SelfTuning())),
     dict(name="clustered20k_p10", gen=lambda: clustered(20000, 2),
          kw=dict(expansion_order=10, leaf_size_source=64, multipole_acceptance=0.5)),
+    # the lane kernel's highest order
+    dict(name="uniform6k_p12", gen=lambda: uniform(6000, 8), kw=dict(expansion_order=12, leaf_size_source=40,
+                                                                     multipole_acceptance=0.5,
+                                                                     scalar_potential=True)),
     # low orders run the thread-per-pair M2L; leaves of ~5 bodies split the P2P lanes over sources
     dict(name="uniform8k_p3_ls5", gen=lambda: uniform(8000, 4), kw=dict(expansion_order=3, leaf_size_source=5,
                                                                        multipole_acceptance=0.6,
@@ -159,6 +163,20 @@ def test_vortex_low_order_and_large_leaves(ctx, p, ls):
         np.testing.assert_allclose(out[:, rows], ref["out"][:, rows], rtol=0, atol=1e-10 * scale)
 
 
+@pytest.mark.parametrize("p", [4, 6, 9, 10])
+def test_vortex_lane_m2l_orders_match_oracle(ctx, p):
+    # plain vortex M2L from order 4 runs the lane-per-pair Lamb-Helmholtz kernel, one template
+    # instance per order; degrees >= 8 stage more rows than a warp has lanes
+    buf = ring(8000, 10 + p)
+    og, oo = opt_pair(expansion_order=p, leaf_size_source=30, multipole_acceptance=0.5, hessian=True)
+    out, res = fm.solve_buffers(buf, L.FMM_POINT_VORTEX, og, ctx=ctx)
+    assert res.n_m2l > 0
+    ref = O.fmm(buf, O.POINT_VORTEX, oo)
+    for rows in (slice(4, 7), slice(7, 16)):
+        scale = np.abs(ref["out"][:, rows]).max()
+        np.testing.assert_allclose(out[:, rows], ref["out"][:, rows], rtol=0, atol=1e-10 * scale)
+
+
 def test_mixed_vortex_matches_f64(ctx):
     # FP32 near field (batch sums promoted to FP64): relative L2 deviation from the FP64 solve below 1e-5
     buf = ring(20000, 7)
@@ -175,7 +193,8 @@ def test_mixed_vortex_matches_f64(ctx):
 @pytest.mark.parametrize("p", [4, 12])
 def test_mixed_vortex_far_field_matches_f64(ctx, p):
     # far field only: the mixed path's lane-per-pair Lamb-Helmholtz M2L (FP32 rotations of
-    # scaled multipoles) against the FP64 engine, velocity and velocity gradient
+    # scaled multipoles) against its FP64 instance (pinned to the oracle above), velocity and
+    # velocity gradient
     buf = ring(30000, 9)
     outs = {}
     for prec in ("f64", "mixed"):
