@@ -259,6 +259,55 @@ __device__ __forceinline__ void packed_batch(const float4* __restrict__ B4, int 
   }
 }
 
+// one source body on one target, vortex particles with the velocity gradient (FP64 path):
+// velocity into u[0..2] (GS); the gradient as Q_ij += d_i (G x d)_j / r^5 and E_k += G_k / r^3,
+// which the caller combines to -3 Q_ij + eps_jki E_k (r^2 / r^5 = 1 / r^3)
+template <class R, bool GS>
+__device__ __forceinline__ void vortex_pair_qe(R tx, R ty, R tz, R sx, R sy, R sz, R s0, R s1, R s2, R* u,
+                                               R (&Q)[9], R (&E)[3]) {
+  const R dx = tx - sx, dy = ty - sy, dz = tz - sz;
+  const R r2 = dx * dx + dy * dy + dz * dz;
+  if (r2 > R(0)) {
+    const R rinv = rsq(r2);
+    const R rinv2 = rinv * rinv;
+    const R den = rinv * rinv2;
+    const R cx = s1 * dz - s2 * dy, cy = s2 * dx - s0 * dz, cz = s0 * dy - s1 * dx;
+    if (GS) {
+      u[0] += cx * den;
+      u[1] += cy * den;
+      u[2] += cz * den;
+    }
+    const R d5 = den * rinv2;
+    const R px = dx * d5, py = dy * d5, pz = dz * d5;
+    Q[0] += px * cx;
+    Q[1] += px * cy;
+    Q[2] += px * cz;
+    Q[3] += py * cx;
+    Q[4] += py * cy;
+    Q[5] += py * cz;
+    Q[6] += pz * cx;
+    Q[7] += pz * cy;
+    Q[8] += pz * cz;
+    E[0] += s0 * den;
+    E[1] += s1 * den;
+    E[2] += s2 * den;
+  }
+}
+
+// the gradient channels g[0..8] (column-major d u_j / d x_i at 3 i + j) from Q and E
+template <class R>
+__device__ __forceinline__ void vortex_grad_from_qe(const R (&Q)[9], const R (&E)[3], R* g) {
+  g[0] = R(-3) * Q[0];
+  g[1] = R(-3) * Q[1] + E[2];
+  g[2] = R(-3) * Q[2] - E[1];
+  g[3] = R(-3) * Q[3] - E[2];
+  g[4] = R(-3) * Q[4];
+  g[5] = R(-3) * Q[5] + E[0];
+  g[6] = R(-3) * Q[6] + E[1];
+  g[7] = R(-3) * Q[7] - E[0];
+  g[8] = R(-3) * Q[8];
+}
+
 // f32x2 with both halves negated
 __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
 
@@ -357,6 +406,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
   constexpr bool MIXED = sizeof(R) == 4;
   constexpr bool PACK = packed<R, KIND>();
   constexpr bool PACKV = packed_vortex<R, KIND>();
+  // unpacked vortex particles with the gradient (the FP64 path) sum it as two parts per target
+  constexpr bool QE = !PACKV && KIND == FMM_POINT_VORTEX && HS;
+  static_assert(!QE || !MIXED, "the mixed vortex path is the packed one");
   static_assert((!PACK && !PACKV) || kTPT == 2, "packed paths pair two targets per lane");
   extern __shared__ __align__(16) unsigned char p2p_smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -394,6 +446,13 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
     for (int k = 0; k < kTPT; ++k)
 #pragma unroll
       for (int a = 0; a < NA; ++a) part[k][a] = R(0), tot[k][a] = 0.0;
+    R Qs[kTPT][9], Es[kTPT][3];  // FP64 vortex gradient as two sums (QE)
+#pragma unroll
+    for (int k = 0; k < kTPT; ++k) {
+#pragma unroll
+      for (int a = 0; a < 9; ++a) Qs[k][a] = R(0);
+      Es[k][0] = Es[k][1] = Es[k][2] = R(0);
+    }
     int lb = l0 + (RW ? 0 : w), poff = 0;  // next source leaf of this warp, bodies of it already taken
     while (lb < l1) {
       // candidate leaves lb + kWarps * lane; take the longest prefix that fits the batch
@@ -520,6 +579,14 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
           part[0][a] += (R)acc[a].x;
           part[1][a] += (R)acc[a].y;
         }
+      } else if constexpr (QE) {
+        for (int j = slice; j < nb; j += SS) {
+          const R sx = B[j], sy = B[NB + j], sz = B[2 * NB + j], s0 = B[3 * NB + j];
+          const R s1 = B[(4 % NV) * NB + j], s2 = B[(5 % NV) * NB + j];
+#pragma unroll
+          for (int k = 0; k < kTPT; ++k)
+            vortex_pair_qe<R, GS>(tx[k], ty[k], tz[k], sx, sy, sz, s0, s1, s2, part[k], Qs[k], Es[k]);
+        }
       } else {
         for (int j = slice; j < nb; j += SS) {
           const R sx = B[j], sy = B[NB + j], sz = B[2 * NB + j], s0 = B[3 * NB + j];
@@ -537,6 +604,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
 #pragma unroll
           for (int a = 0; a < NA; ++a) tot[k][a] += (double)part[k][a], part[k][a] = R(0);
       }
+    }
+    if constexpr (QE) {
+#pragma unroll
+      for (int k = 0; k < kTPT; ++k) vortex_grad_from_qe<R>(Qs[k], Es[k], &part[k][(GS ? 3 : 0) % NA]);
     }
     if (!MIXED) {
 #pragma unroll
