@@ -443,8 +443,10 @@ def vjp(system, d_potential=None, d_velocity=None, targets=None, *, leaf_size=20
 
 class Server:
     """Concurrent fmm! requests on one device (fmm_serve_*): ``n_workers`` solver
-    contexts run queued requests as soon as one finishes; each worker's HBM budget
-    is ``hbm_budget / n_workers`` (0: unlimited)."""
+    contexts run queued requests (oldest first) as soon as one finishes, and
+    ``n_workers // 2`` (at least one) express contexts on highest-priority streams run
+    requests of at most 65,536 source plus target bodies; each of these workers has an
+    HBM budget of ``hbm_budget / (n_workers + n_workers // 2)`` (0: unlimited)."""
 
     def __init__(self, n_workers=4, hbm_budget=0, ctx=None):
         self.ctx = ctx or default_context()

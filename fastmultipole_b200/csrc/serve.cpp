@@ -1,10 +1,13 @@
 // serve.cpp -- concurrent request serving on one device (fmm_serve_*).
 //
-// n_workers threads, each owning a solver context (its own non-blocking stream,
-// trees, lists and scratch) on the serving context's device; a FIFO queue of
-// requests; a worker runs fmm_solve on the next request as soon as it finishes
-// one, so small requests overlap on the GPU instead of queueing behind each other.
-// Results are kept until polled.
+// n_workers general workers and n_workers / 2 (at least one) express workers, each a
+// thread owning a solver context (its own non-blocking stream, trees, lists and
+// scratch) on the serving context's device, and one queue of requests in arrival
+// order.  A general worker takes the oldest queued request; an express worker takes the
+// oldest request of at most kExpressBodies source plus target bodies and runs it on a
+// highest-priority stream, so that small requests neither wait for a worker behind
+// large ones nor queue for SMs behind their kernels.  A worker takes its next request
+// as soon as it finishes one.  Results are kept until polled.
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -29,10 +32,18 @@ struct Done {
   fmm_result result;
 };
 
+constexpr int64_t kExpressBodies = 65536;
+
+struct Job {
+  uint64_t id;
+  fmm_request req;
+  int64_t size;  // source + target bodies
+};
+
 struct Server {
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
-  std::deque<std::pair<uint64_t, fmm_request>> queue;
+  std::deque<Job> queue;  // arrival order
   std::unordered_map<uint64_t, Done> done;
   uint64_t next_id = 1;
   bool stopping = false;
@@ -41,22 +52,28 @@ struct Server {
   std::vector<cudaStream_t> streams;
 };
 
-void worker_loop(Server* S, fmm_ctx* c) {
+void worker_loop(Server* S, fmm_ctx* c, bool express) {
   for (;;) {
-    std::pair<uint64_t, fmm_request> job;
+    Job job;
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      S->cv_work.wait(lk, [&] { return S->stopping || !S->queue.empty(); });
-      if (S->queue.empty()) return;  // stopping and drained
-      job = S->queue.front();
-      S->queue.pop_front();
+      size_t pick = 0;
+      auto eligible = [&] {
+        for (pick = 0; pick < S->queue.size(); ++pick)
+          if (!express || S->queue[pick].size <= kExpressBodies) return true;
+        return false;
+      };
+      S->cv_work.wait(lk, [&] { return S->stopping || eligible(); });
+      if (!eligible()) return;  // stopping, and nothing left for this worker
+      job = S->queue[pick];
+      S->queue.erase(S->queue.begin() + (std::ptrdiff_t)pick);
     }
     Done d;
     std::memset(&d.result, 0, sizeof(d.result));
-    d.status = fmm_solve(c, &job.second.target, &job.second.source, &job.second.options, &d.result);
+    d.status = fmm_solve(c, &job.req.target, &job.req.source, &job.req.options, &d.result);
     {
       std::lock_guard<std::mutex> lk(S->mu);
-      S->done[job.first] = d;
+      S->done[job.id] = d;
     }
     S->cv_done.notify_all();
   }
@@ -72,13 +89,21 @@ int fmm_serve_start(fmm_ctx* ctx, int n_workers, size_t hbm_budget_bytes) {
   if (slot) return FMM_OK;  // already serving
   Server* S = new Server();
   const int dev = fmmb::ctx_device(ctx);
-  for (int w = 0; w < n_workers; ++w) {
+  const int n_express = n_workers / 2 > 0 ? n_workers / 2 : 1, n_all = n_workers + n_express;
+  int least = 0, greatest = 0;
+  if (cudaSetDevice(dev) != cudaSuccess || cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) {
+    delete S;
+    return FMM_ERR_CUDA;
+  }
+  for (int w = 0; w < n_all; ++w) {
     fmm_ctx* c = nullptr;
     int rc = fmm_ctx_create(&c, dev);
     cudaStream_t st = nullptr;
-    if (rc == FMM_OK && cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) rc = FMM_ERR_CUDA;
+    if (rc == FMM_OK &&
+        cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, w < n_workers ? least : greatest) != cudaSuccess)
+      rc = FMM_ERR_CUDA;
     if (rc == FMM_OK) rc = fmm_ctx_set_stream(c, st);
-    if (rc == FMM_OK && hbm_budget_bytes) rc = fmm_ctx_set_hbm_budget(c, hbm_budget_bytes / n_workers);
+    if (rc == FMM_OK && hbm_budget_bytes) rc = fmm_ctx_set_hbm_budget(c, hbm_budget_bytes / n_all);
     if (rc != FMM_OK) {
       if (c) fmm_ctx_destroy(c);
       if (st) cudaStreamDestroy(st);
@@ -92,7 +117,7 @@ int fmm_serve_start(fmm_ctx* ctx, int n_workers, size_t hbm_budget_bytes) {
     S->ctxs.push_back(c);
     S->streams.push_back(st);
   }
-  for (int w = 0; w < n_workers; ++w) S->workers.emplace_back(worker_loop, S, S->ctxs[w]);
+  for (int w = 0; w < n_all; ++w) S->workers.emplace_back(worker_loop, S, S->ctxs[w], w >= n_workers);
   slot = S;
   return FMM_OK;
 }
@@ -105,9 +130,10 @@ int fmm_serve_submit(fmm_ctx* ctx, const fmm_request* request, uint64_t* id) {
     std::lock_guard<std::mutex> lk(S->mu);
     if (S->stopping) return FMM_ERR_STATE;
     *id = S->next_id++;
-    S->queue.emplace_back(*id, *request);
+    const int64_t nt = request->target.positions ? request->target.n_bodies : 0;
+    S->queue.push_back(Job{*id, *request, request->source.n_bodies + nt});
   }
-  S->cv_work.notify_one();
+  S->cv_work.notify_all();  // general and express workers wait for different requests
   return FMM_OK;
 }
 

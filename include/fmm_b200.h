@@ -200,8 +200,11 @@ FMM_API int fmm_vjp(fmm_ctx* ctx, const fmm_target_system* target, const fmm_sou
  * The reference reuses a Cache across fmm! calls (src/containers.jl:264-292) and runs
  * one call at a time.  A serving context keeps n_workers solver contexts, each with
  * its own stream and resident buffers, and runs queued requests concurrently: a
- * worker takes the next request as soon as it finishes one.  Each worker's HBM
- * budget is hbm_budget_bytes / n_workers (0 = unlimited); a request that does not fit
+ * worker takes the oldest queued request as soon as it finishes one.  n_workers / 2
+ * (at least one) express workers besides take only requests of at most 65,536 source
+ * plus target bodies, on highest-priority streams, so that small requests do not wait
+ * behind large ones.  Each of the n_workers + n_workers / 2 workers has an HBM
+ * budget of hbm_budget_bytes / their number (0 = unlimited); a request that does not fit
  * finishes with FMM_ERR_MEMORY.  A request's result does not depend on what else is
  * running (each request runs the deterministic fmm_solve path on its own buffers).
  * The caller keeps every buffer of a request alive until fmm_serve_poll has

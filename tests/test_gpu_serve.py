@@ -86,7 +86,7 @@ def test_pending_errors_and_budget():
         if rc == L.FMM_PENDING:
             rc, out, _ = server.poll(rid, timeout_ms=-1)
         assert rc == L.FMM_OK and np.isfinite(out[:, 4:7]).all()
-        # a request above one worker's share of the budget (1 GB) fails alone
+        # a request above one worker's share of the budget (2 GB over 2 + 1 workers) fails alone
         huge = bodies(4_000_000, 1, 12)
         rid = server.submit(huge, 1, opt)
         assert server.poll(rid)[0] == L.FMM_ERR_MEMORY
