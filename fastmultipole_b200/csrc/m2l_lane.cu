@@ -1230,15 +1230,17 @@ struct L2LLaneGo {
 // then gives the local sets times t^(n+1) and t^(n+2), on which the Lamb-Helmholtz coupling
 // of transform_lamb_helmholtz_local! (src/translate.jl:98-142) needs no power of t:
 //   phi(n, m) -= i (m / n) chi(n, m),  chi(n, m) -= chi(n + 1, m) / (n + 1).
-// The rotated-back degrees are scaled by t^-(n+1) / t^-(n+2) in FP64 and summed over the
-// lanes through shared memory into the warp's FP64 accumulator.
+// The rotated-back degrees are staged in shared memory unscaled (in V) with each lane's
+// t^-(n+1) / t^-(n+2), and summed over the lanes in FP64, value times power, into the warp's
+// FP64 accumulator: an FP32 stage keeps the warp's shared memory at order 12 to 55.5 KB
+// (4 CTAs per SM instead of 3 with an FP64 stage).
 template <class V>
 __device__ __forceinline__ V& MSl(V* Ms, int i, int c, int lane) { return Ms[(4 * i + c) * 32 + lane]; }
 
 template <int PMAX, class V>
 constexpr size_t lane_lh_smem_bytes() {
-  return ((size_t)4 * (PMAX + 1) * 33 + (size_t)4 * hi(PMAX + 1, 0)) * sizeof(double) +
-         (size_t)4 * hi(PMAX + 1, 0) * 32 * sizeof(V);
+  return ((size_t)4 * hi(PMAX + 1, 0) + 64) * sizeof(double) +
+         ((size_t)4 * (PMAX + 1) * 33 + (size_t)4 * hi(PMAX + 1, 0) * 32) * sizeof(V);
 }
 
 // coaxial translation of one set (c0 = 0 or 2) of degree n, scaled: sum_{n'} (n+n')! M(n', m)
@@ -1270,9 +1272,10 @@ __global__ void __launch_bounds__(32) k_m2l_lane_lh(const int* __restrict__ tgt_
                                                     unsigned long long* __restrict__ st_flops) {
   constexpr int NH = hi(PMAX + 1, 0);
   extern __shared__ double lane_smem[];
-  double* stage = lane_smem;                   // [4 (PMAX+1)][33]
-  double* acc = stage + 4 * (PMAX + 1) * 33;   // [4 NH]
-  V* Ms = reinterpret_cast<V*>(acc + 4 * NH);  // rotated multipole [4 NH][32]
+  double* acc = lane_smem;                    // [4 NH]
+  double* tsc = acc + 4 * NH;                 // per lane t^-(n+1), t^-(n+2): [2][32]
+  V* stage = reinterpret_cast<V*>(tsc + 64);  // unscaled rotated-back values [4 (PMAX+1)][33]
+  V* Ms = stage + 4 * (PMAX + 1) * 33;        // rotated multipole [4 NH][32]
   const int lane = threadIdx.x;
   const int b = blockIdx.x;
   const int t = tgt_list[b];
@@ -1379,8 +1382,8 @@ __global__ void __launch_bounds__(32) k_m2l_lane_lh(const int* __restrict__ tgt_
         if (m > n) break;
         const V vr = Yr[m] * er + Yi[m] * ei;  // times e^{-i m phi}
         const V vi = Yi[m] * er - Yr[m] * ei;
-        stage[(4 * m) * 33 + lane] = valid ? vr * tn1 : 0.0;
-        stage[(4 * m + 1) * 33 + lane] = valid ? vi * tn1 : 0.0;
+        stage[(4 * m) * 33 + lane] = valid ? vr : V(0);
+        stage[(4 * m + 1) * 33 + lane] = valid ? vi : V(0);
         const V tt = er;
         er = er * fcph - ei * fsph;
         ei = tt * fsph + ei * fcph;
@@ -1401,18 +1404,22 @@ __global__ void __launch_bounds__(32) k_m2l_lane_lh(const int* __restrict__ tgt_
         if (m > n) break;
         const V vr = Yr[m] * er + Yi[m] * ei;
         const V vi = Yi[m] * er - Yr[m] * ei;
-        stage[(4 * m + 2) * 33 + lane] = valid ? vr * tn2 : 0.0;
-        stage[(4 * m + 3) * 33 + lane] = valid ? vi * tn2 : 0.0;
+        stage[(4 * m + 2) * 33 + lane] = valid ? vr : V(0);
+        stage[(4 * m + 3) * 33 + lane] = valid ? vi : V(0);
         const V tt = er;
         er = er * fcph - ei * fsph;
         ei = tt * fsph + ei * fcph;
       }
+      tsc[lane] = tn1;
+      tsc[32 + lane] = tn2;
       __syncwarp();
-      // 4 (n + 1) staged rows: more than the warp's 32 lanes from degree 8
+      // 4 (n + 1) staged rows: more than the warp's 32 lanes from degree 8; each value times
+      // its lane's power of t in FP64 (set 0: t^-(n+1), set 1: t^-(n+2))
       for (int row = lane; row < 4 * (n + 1); row += 32) {
+        const double* sc = tsc + ((row & 2) ? 32 : 0);
         double v = 0.0;
 #pragma unroll 8
-        for (int k = 0; k < 32; ++k) v += stage[row * 33 + k];
+        for (int k = 0; k < 32; ++k) v += (double)stage[row * 33 + k] * sc[k];
         acc[4 * hi(n, 0) + row] += v;
       }
       __syncwarp();
