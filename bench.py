@@ -103,7 +103,7 @@ WORKLOADS = {
 
 # DRAM bytes (read + write) of the solve's near-field launch, one ncu capture of the full-size
 # workload (dram__bytes_read.sum + dram__bytes_write.sum)
-NEAR_TRAFFIC = {"c2": 311889408 + 46925568}
+NEAR_TRAFFIC = {"c2": 311889408 + 46925568, "c3": 5638054144 + 197501696}
 
 
 def options(fm, w, precision):
