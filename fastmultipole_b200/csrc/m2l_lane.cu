@@ -414,34 +414,46 @@ __device__ __forceinline__ double fwd_degree_f(int n, const Pair& q, float* Ms, 
 
 // local error estimate of degree n (eps_local above) from the scaled rotated multipole;
 // tn1 = t^-(n+1)
+// (the coaxial sums run source degrees outer, orders inner, so that one degree's loads and
+// FMAs are independent; each sum keeps its n'-ascending order)
+template <int PMAX>
 __device__ __forceinline__ double eps_local_f(int n, const Pair& q, const float* Ms, int lane, bool power,
                                               double tn1) {
   if (power) {
-    double a = 0.0;
+    double vr[PMAX + 1], vi[PMAX + 1];
+#pragma unroll
+    for (int m = 0; m <= PMAX; ++m) vr[m] = vi[m] = 0.0;
 #pragma unroll 1
-    for (int m = 0; m <= n; ++m) {
-      double vr = 0, vi = 0;
-#pragma unroll 1
-      for (int np = m; np <= n; ++np) {
-        const double c = c_fact[n + np];
-        vr += c * MSfr(Ms, hi(np, m), 0, lane);
-        vi += c * MSfr(Ms, hi(np, m), 1, lane);
+    for (int np = 0; np <= n; ++np) {
+      const double c = c_fact[n + np];
+      const int base = hi(np, 0);
+#pragma unroll
+      for (int m = 0; m <= PMAX; ++m) {
+        if (m > np) break;
+        vr[m] += c * MSfr(Ms, base + m, 0, lane);
+        vi[m] += c * MSfr(Ms, base + m, 1, lane);
       }
-      vr *= tn1;
-      vi *= tn1;
+    }
+    double a = 0.0;
+#pragma unroll
+    for (int m = 0; m <= PMAX; ++m) {
+      if (m > n) break;
+      const double xr = vr[m] * tn1, xi = vi[m] * tn1;
       const double Nt = c_Lt[hi(n, m)];
-      a += (vr * vr + vi * vi) * Nt * Nt;
+      a += (xr * xr + xi * xi) * Nt * Nt;
     }
     const double lphi = sqrt(a);
     return 1.7320508075688772 * lphi * q.r_l_nm1 * q.nm1_fact_inv / c_Lt[hi(n, 0)];
   }
   double a0 = 0, b1r = 0, b1i = 0;
 #pragma unroll 1
-  for (int np = 0; np <= n; ++np) a0 += c_fact[n + np] * MSfr(Ms, hi(np, 0), 0, lane);
-#pragma unroll 1
-  for (int np = 1; np <= n; ++np) {
-    b1r += c_fact[n + np] * MSfr(Ms, hi(np, 1), 0, lane);
-    b1i += c_fact[n + np] * MSfr(Ms, hi(np, 1), 1, lane);
+  for (int np = 0; np <= n; ++np) {
+    const double c = c_fact[n + np];
+    a0 += c * MSfr(Ms, hi(np, 0), 0, lane);
+    if (np >= 1) {
+      b1r += c * MSfr(Ms, hi(np, 1), 0, lane);
+      b1i += c * MSfr(Ms, hi(np, 1), 1, lane);
+    }
   }
   return (fabs(b1r * tn1) + fabs(b1i * tn1) + fabs(a0 * tn1)) * q.r_l_nm1 * q.nm1_fact_inv;
 }
@@ -456,7 +468,7 @@ __device__ __forceinline__ void err_step_f(int n, Pair& q, const float* Ms, int 
   else
     eps_mp = (sqrt(y1r * y1r + y1i * y1i) + fabs(y0r)) * q.np1_fact * q.r_mp_inv_np2;
   if (eps_mp <= q.thr) {
-    const double eps_l = eps_local_f(n, q, Ms, lane, power, tn1);
+    const double eps_l = eps_local_f<PMAX>(n, q, Ms, lane, power, tn1);
     if (eps_mp + eps_l * 2.0 <= q.thr) {
       q.P = n - 1 + (be ? 1 : 0);
       q.ok = true;
@@ -483,21 +495,22 @@ template <int PMAX>
 __device__ __forceinline__ void back_degree_f(int n, const Pair& q, const float* Ms, double* stage, double* acc,
                                               int lane, double tn1) {
   const bool on = q.valid && n <= q.P;
+  // out(n, m) = sum_{n' >= m} (n + n')! M(n', m): source degrees outer, orders inner, so that
+  // one degree's loads and FMAs are independent (each sum keeps its n'-ascending order)
   float Xr[PMAX + 1], Xi[PMAX + 1];
 #pragma unroll
-  for (int m = 0; m <= PMAX; ++m) {
-    Xr[m] = Xi[m] = 0.0f;
-    if (m > n) continue;
-    float vr = 0, vi = 0;
-    const int top = on ? q.P : m - 1;
+  for (int m = 0; m <= PMAX; ++m) Xr[m] = Xi[m] = 0.0f;
+  const int top = on ? q.P : -1;
 #pragma unroll 1
-    for (int np = m; np <= top; ++np) {
-      const float c = c_factF[n + np];
-      vr += c * MSfr(Ms, hi(np, m), 0, lane);
-      vi += c * MSfr(Ms, hi(np, m), 1, lane);
+  for (int np = 0; np <= top; ++np) {
+    const float c = c_factF[n + np];
+    const int base = hi(np, 0);
+#pragma unroll
+    for (int m = 0; m <= PMAX; ++m) {
+      if (m > n || m > np) break;
+      Xr[m] += c * MSfr(Ms, base + m, 0, lane);
+      Xi[m] += c * MSfr(Ms, base + m, 1, lane);
     }
-    Xr[m] = vr;
-    Xi[m] = vi;
   }
   float Yr[PMAX + 1], Yi[PMAX + 1];
   rot_y<PMAX, true, float>(n, Xr, Xi, (float)q.cth, (float)q.sth, Yr, Yi);
@@ -1247,19 +1260,20 @@ constexpr size_t lane_lh_smem_bytes() {
 template <int PMAX, class V>
 __device__ __forceinline__ void coax_lh(int n, int P, const V* Ms, int c0, int lane, V (&Xr)[PMAX + 1],
                                         V (&Xi)[PMAX + 1]) {
+  // source degrees outer, orders inner: one degree's loads and FMAs are independent (each
+  // sum keeps its n'-ascending order)
 #pragma unroll
-  for (int m = 0; m <= PMAX; ++m) {
-    Xr[m] = Xi[m] = V(0);
-    if (m > n) continue;
-    V vr = 0, vi = 0;
+  for (int m = 0; m <= PMAX; ++m) Xr[m] = Xi[m] = V(0);
 #pragma unroll 1
-    for (int np = m; np <= P; ++np) {
-      const V c = sizeof(V) == 4 ? (V)c_factF[n + np] : (V)c_fact[n + np];
-      vr += c * Ms[(4 * hi(np, m) + c0) * 32 + lane];
-      vi += c * Ms[(4 * hi(np, m) + c0 + 1) * 32 + lane];
+  for (int np = 0; np <= P; ++np) {
+    const V c = sizeof(V) == 4 ? (V)c_factF[n + np] : (V)c_fact[n + np];
+    const int base = hi(np, 0);
+#pragma unroll
+    for (int m = 0; m <= PMAX; ++m) {
+      if (m > n || m > np) break;
+      Xr[m] += c * Ms[(4 * (base + m) + c0) * 32 + lane];
+      Xi[m] += c * Ms[(4 * (base + m) + c0 + 1) * 32 + lane];
     }
-    Xr[m] = vr;
-    Xi[m] = vi;
   }
 }
 
