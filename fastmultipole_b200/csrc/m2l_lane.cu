@@ -235,25 +235,35 @@ __device__ __forceinline__ double fwd_degree(int n, const Pair& q, double* Ms, i
 }
 
 // local error estimate of degree n from the rotated multipole of degrees <= n
+// The coaxial factor of source degree n' is the running product n!/t^(n+1) * prod_{j<=n'}
+// (n+j)/t in the reference's order whatever the order m, so the sums run source degrees
+// outer and orders inner (one degree's loads and FMAs independent; each sum keeps its
+// n'-ascending order).
+template <int PMAX>
 __device__ __forceinline__ double eps_local(int n, const Pair& q, const double* Ms, int lane, bool power) {
   if (power) {
     // degree n of translate_multipole_to_local_z_n! and local_power (src/translate.jl:238-295, :455-502)
-    double a = 0.0, cs = q.un;
+    double vr[PMAX + 1], vi[PMAX + 1];
+#pragma unroll
+    for (int m = 0; m <= PMAX; ++m) vr[m] = vi[m] = 0.0;
+    double c = q.un;
 #pragma unroll 1
-    for (int m = 0; m <= n; ++m) {
-      if (m > 0) cs *= (n + m) * q.rinv;  // (n + m)! / t^(n+m+1), the reference's product order
-      double c = cs;
-      int n_np = n + m;
-      double vr = 0, vi = 0;
-#pragma unroll 1
-      for (int np = m; np <= n; ++np) {
-        vr += c * MSr(Ms, hi(np, m), 0, lane);
-        vi += c * MSr(Ms, hi(np, m), 1, lane);
-        n_np += 1;
-        c *= n_np * q.rinv;
+    for (int np = 0; np <= n; ++np) {
+      if (np > 0) c *= (n + np) * q.rinv;  // (n + n')! / t^(n+n'+1), the reference's product order
+      const int base = hi(np, 0);
+#pragma unroll
+      for (int m = 0; m <= PMAX; ++m) {
+        if (m > np) break;
+        vr[m] += c * MSr(Ms, base + m, 0, lane);
+        vi[m] += c * MSr(Ms, base + m, 1, lane);
       }
+    }
+    double a = 0.0;
+#pragma unroll
+    for (int m = 0; m <= PMAX; ++m) {
+      if (m > n) break;
       const double Nt = c_Lt[hi(n, m)];
-      a += (vr * vr + vi * vi) * Nt * Nt;
+      a += (vr[m] * vr[m] + vi[m] * vi[m]) * Nt * Nt;
     }
     const double lphi = sqrt(a);
     return 1.7320508075688772 * lphi * q.r_l_nm1 * q.nm1_fact_inv / c_Lt[hi(n, 0)];
@@ -293,7 +303,7 @@ __device__ __forceinline__ void err_step(int n, Pair& q, const double* Ms, int l
   else
     eps_mp = (sqrt(y1r * y1r + y1i * y1i) + fabs(y0r)) * q.np1_fact * q.r_mp_inv_np2;
   if (eps_mp <= q.thr) {
-    const double eps_l = eps_local(n, q, Ms, lane, power);
+    const double eps_l = eps_local<PMAX>(n, q, Ms, lane, power);
     if (eps_mp + eps_l * 2.0 <= q.thr) {
       q.P = n - 1 + (be ? 1 : 0);
       q.ok = true;
@@ -321,26 +331,23 @@ template <int PMAX>
 __device__ __forceinline__ void back_degree(int n, double un, const Pair& q, const double* Ms, double* stage,
                                             double* acc, int lane) {
   const bool on = q.valid && n <= q.P;
+  // (n + n')! / t^(n+n'+1) as one running product in the reference's order, common to every
+  // order m: source degrees outer, orders inner
   double Xr[PMAX + 1], Xi[PMAX + 1];
-  double cs = un;
 #pragma unroll
-  for (int m = 0; m <= PMAX; ++m) {
-    Xr[m] = Xi[m] = 0.0;
-    if (m > n) continue;
-    if (m > 0) cs *= (n + m) * q.rinv;  // (n + m)! / t^(n+m+1), the reference's product order
-    double c = cs;
-    int n_np = n + m;
-    double vr = 0, vi = 0;
-    const int top = on ? q.P : m - 1;
+  for (int m = 0; m <= PMAX; ++m) Xr[m] = Xi[m] = 0.0;
+  const int top = on ? q.P : -1;
+  double c = un;
 #pragma unroll 1
-    for (int np = m; np <= top; ++np) {
-      vr += c * MSr(Ms, hi(np, m), 0, lane);
-      vi += c * MSr(Ms, hi(np, m), 1, lane);
-      n_np += 1;
-      c *= n_np * q.rinv;
+  for (int np = 0; np <= top; ++np) {
+    if (np > 0) c *= (n + np) * q.rinv;
+    const int base = hi(np, 0);
+#pragma unroll
+    for (int m = 0; m <= PMAX; ++m) {
+      if (m > n || m > np) break;
+      Xr[m] += c * MSr(Ms, base + m, 0, lane);
+      Xi[m] += c * MSr(Ms, base + m, 1, lane);
     }
-    Xr[m] = vr;
-    Xi[m] = vi;
   }
   double Yr[PMAX + 1], Yi[PMAX + 1];
   rot_y<PMAX, true>(n, Xr, Xi, q.cth, q.sth, Yr, Yi);
@@ -832,24 +839,27 @@ __global__ void __launch_bounds__(32) k_m2m_lane(int l0, int l1, const int* __re
       MS(Ms, hi(n, m), 0, lane) = Yr[m];
       MS(Ms, hi(n, m), 1, lane) = Yi[m];
     }
-    // translate_multipole_z!: out(n, m) = sum_{n' = n..m} (-t)^(n-n') / (n-n')! M(n', m)
+    // translate_multipole_z!: out(n, m) = sum_{n' = n..m} (-t)^(n-n') / (n-n')! M(n', m); the
+    // factor depends on n - n' only: source degrees outer (descending), orders inner
 #pragma unroll
-    for (int m = 0; m <= PMAX; ++m) {
-      Xr[m] = Xi[m] = 0.0;
-      if (m > n) continue;
-      double f = 1.0, tp = 1.0, vr = 0.0, vi = 0.0;
+    for (int m = 0; m <= PMAX; ++m) Xr[m] = Xi[m] = 0.0;
+    {
+      double f = 1.0, tp = 1.0;
       int q = 1;
 #pragma unroll 1
-      for (int np = n; np >= m; --np) {
+      for (int np = n; np >= 0; --np) {
         const double cc = tp / f;
-        vr += cc * MSr(Ms, hi(np, m), 0, lane);
-        vi += cc * MSr(Ms, hi(np, m), 1, lane);
+        const int base = hi(np, 0);
+#pragma unroll
+        for (int m = 0; m <= PMAX; ++m) {
+          if (m > np) break;
+          Xr[m] += cc * MSr(Ms, base + m, 0, lane);
+          Xi[m] += cc * MSr(Ms, base + m, 1, lane);
+        }
         tp *= mt;
         f *= q;
         q += 1;
       }
-      Xr[m] = vr;
-      Xi[m] = vi;
     }
     rot_y<PMAX, false>(n, Xr, Xi, g.cth, g.sth, Yr, Yi);
     rotz_back<PMAX>(n, g, Yr, Yi);
@@ -904,23 +914,26 @@ __global__ void __launch_bounds__(32) k_l2l_lane(int c0, int c1, const int* __re
   }
 #pragma unroll 1
   for (int n = 0; n <= PMAX; ++n) {
-    // translate_local_z!: out(n, m) = sum_{n' = n..P} prod_{q=1}^{n'-n} (-t / q) L(n', m)
+    // translate_local_z!: out(n, m) = sum_{n' = n..P} prod_{q=1}^{n'-n} (-t / q) L(n', m); the
+    // factor depends on n' - n only: source degrees outer, orders inner
     double Xr[PMAX + 1], Xi[PMAX + 1], Yr[PMAX + 1], Yi[PMAX + 1];
 #pragma unroll
-    for (int m = 0; m <= PMAX; ++m) {
-      Xr[m] = Xi[m] = 0.0;
-      if (m > n) continue;
-      double cc = 1.0, vr = 0.0, vi = 0.0;
+    for (int m = 0; m <= PMAX; ++m) Xr[m] = Xi[m] = 0.0;
+    {
+      double cc = 1.0;
       int q = 1;
 #pragma unroll 1
       for (int np = n; np <= PMAX; ++np) {
-        vr += cc * MSr(Ls, hi(np, m), 0, lane);
-        vi += cc * MSr(Ls, hi(np, m), 1, lane);
+        const int base = hi(np, 0);
+#pragma unroll
+        for (int m = 0; m <= PMAX; ++m) {
+          if (m > n) break;
+          Xr[m] += cc * MSr(Ls, base + m, 0, lane);
+          Xi[m] += cc * MSr(Ls, base + m, 1, lane);
+        }
         cc *= mt / q;
         q += 1;
       }
-      Xr[m] = vr;
-      Xi[m] = vi;
     }
     rot_y<PMAX, true>(n, Xr, Xi, g.cth, g.sth, Yr, Yi);
     rotz_back<PMAX>(n, g, Yr, Yi);
