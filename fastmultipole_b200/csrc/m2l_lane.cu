@@ -1277,7 +1277,7 @@ __device__ __forceinline__ void coax_lh(int n, int P, const V* Ms, int c0, int l
   // sum keeps its n'-ascending order)
 #pragma unroll
   for (int m = 0; m <= PMAX; ++m) Xr[m] = Xi[m] = V(0);
-#pragma unroll 1
+#pragma unroll 2
   for (int np = 0; np <= P; ++np) {
     const V c = sizeof(V) == 4 ? (V)c_factF[n + np] : (V)c_fact[n + np];
     const int base = hi(np, 0);
