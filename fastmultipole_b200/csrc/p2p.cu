@@ -132,8 +132,9 @@ __device__ __forceinline__ void store(double* o, const A& acc, int k) {
 }
 
 // ---------------------------------------------------------------------------
-// Direct-list P2P.  One CTA of kWarps warps owns one direct-list row (a target leaf).
-// Each warp takes every kWarps-th source leaf of the leaf's direct-list row and
+// Direct-list P2P.  One CTA of kWarps warps (kWideWarps when the launch has few rows, so
+// that a few long rows still fill the GPU) owns one direct-list row (a target leaf).
+// Each warp takes every W-th source leaf of the leaf's direct-list row and
 // gathers up to batch_bodies() bodies of consecutive leaves of its share (many
 // small leaves, or a piece of a large one) into its own shared-memory batch,
 // converted once per body (to FP32 relative to the target leaf centre on the
@@ -146,6 +147,10 @@ __device__ __forceinline__ void store(double* o, const A& acc, int k) {
 // of small target leaves (at most 8 bodies on average) take one warp each instead of
 // a CTA, so that the per-row setup and the cross-warp sum do not dominate their work.
 constexpr int kWarps = 4;
+// launches of fewer rows than kWideRowsPerSM per SM take kWideWarps warps per row: a few
+// long rows (targets of a dual tree near many sources) would otherwise leave the SMs idle
+constexpr int kWideWarps = 16;
+constexpr int kWideRowsPerSM = 4;
 constexpr int kTPT = 2;
 constexpr unsigned kAll = 0xffffffffu;
 
@@ -393,8 +398,9 @@ __device__ __forceinline__ void packed_vortex_batch(const float4* __restrict__ B
 
 // RW: one warp per row (rows of small leaves, kWarps rows per CTA), the warp adding its
 // sums to the targets itself; otherwise one CTA per row, the warps splitting its sources.
-template <class R, int KIND, bool PS, bool GS, bool HS, bool RW>
-__global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt_list, const int* __restrict__ off,
+// W warps per CTA: kWarps, or kWideWarps for launches of few rows (one long row per CTA).
+template <class R, int KIND, bool PS, bool GS, bool HS, bool RW, int W = kWarps>
+__global__ void __launch_bounds__(W * 32) k_p2p(const int* __restrict__ tgt_list, const int* __restrict__ off,
                                                      int n_rows, const int* __restrict__ src_of,
                                                      const int* __restrict__ t_start, const int* __restrict__ t_count,
                                                      const double* __restrict__ t_center,
@@ -413,10 +419,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
   extern __shared__ __align__(16) unsigned char p2p_smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   R* B = reinterpret_cast<R*>(p2p_smem) + w * NS * NB;  // this warp's batch, plane v at B[v * NB]
-  double* red = reinterpret_cast<double*>(p2p_smem + kWarps * NS * NB * sizeof(R));  // [kWarps][32 kTPT][NA]
-  const int row = RW ? blockIdx.x * kWarps + w : blockIdx.x;
+  double* red = reinterpret_cast<double*>(p2p_smem + W * NS * NB * sizeof(R));  // [W][32 kTPT][NA]
+  const int row = RW ? blockIdx.x * W + w : blockIdx.x;
   if (RW && row >= n_rows) return;  // whole warps: no block barrier on the RW path
-  constexpr int LS = RW ? 1 : kWarps;  // stride of this warp's source leaves along the row
+  constexpr int LS = RW ? 1 : W;  // stride of this warp's source leaves along the row
   const int t = tgt_list[row];
   const int l0 = off[row], l1 = off[row + 1];
   const int ts = t_start[t], tc = t_count[t];
@@ -455,7 +461,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
     }
     int lb = l0 + (RW ? 0 : w), poff = 0;  // next source leaf of this warp, bodies of it already taken
     while (lb < l1) {
-      // candidate leaves lb + kWarps * lane; take the longest prefix that fits the batch
+      // candidate leaves lb + W * lane; take the longest prefix that fits the batch
       const int l = lb + LS * lane;
       int cnt = 0, sb = 0, sl = -1;
       if (l < l1) {
@@ -647,11 +653,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
       }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < nt * NA; e += kWarps * 32) {
+    for (int e = threadIdx.x; e < nt * NA; e += W * 32) {
       const int i = e / NA, a = e - i * NA;
       double v = 0;
 #pragma unroll
-      for (int q = 0; q < kWarps; ++q) v += red[(q * 32 * kTPT + i) * NA + a];
+      for (int q = 0; q < W; ++q) v += red[(q * 32 * kTPT + i) * NA + a];
       if (KIND == FMM_POINT_SOURCE && a == 0 && !PS) continue;
       // atomic: under SelfTuning a non-leaf target branch and its own leaves can both own direct-list rows
       atomicAdd(acc13 + 13 * (int64_t)(ts + tile + i) + chan_row<KIND, GS>(a), v * kOneOver4Pi);
@@ -660,10 +666,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_p2p(const int* __restrict__ tgt
   }
 }
 
-template <class R, int KIND, bool GS, bool HS>
+template <class R, int KIND, bool GS, bool HS, int W = kWarps>
 constexpr size_t p2p_smem_bytes() {
-  return (size_t)kWarps * slots_per_body<R, KIND>() * batch_bodies<R, KIND>() * sizeof(R) +
-         (size_t)kWarps * 32 * kTPT * n_chan<KIND, GS, HS>() * sizeof(double);
+  return (size_t)W * slots_per_body<R, KIND>() * batch_bodies<R, KIND>() * sizeof(R) +
+         (size_t)W * 32 * kTPT * n_chan<KIND, GS, HS>() * sizeof(double);
 }
 
 // all pairs: each CTA owns kP2PThreads*TPT consecutive targets
@@ -740,12 +746,24 @@ void run_p2p(const DevTree& tt, const DevTree& stt, const DevLists& L, double* a
         L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
         stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13);
   } else {
-    if (smem > 48 * 1024)
-      FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2p<R, KIND, PS, GS, HS, false>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_p2p<R, KIND, PS, GS, HS, false><<<rows, kWarps * 32, smem, st>>>(
-        L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
-        stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13);
+    int dev = 0, n_sm = 0;
+    FMM_CUDA_TRY(cudaGetDevice(&dev));
+    FMM_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    if (rows < kWideRowsPerSM * n_sm) {
+      constexpr size_t smw = p2p_smem_bytes<R, KIND, GS, HS, kWideWarps>();
+      FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2p<R, KIND, PS, GS, HS, false, kWideWarps>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw));
+      k_p2p<R, KIND, PS, GS, HS, false, kWideWarps><<<rows, kWideWarps * 32, smw, st>>>(
+          L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
+          stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13);
+    } else {
+      if (smem > 48 * 1024)
+        FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2p<R, KIND, PS, GS, HS, false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_p2p<R, KIND, PS, GS, HS, false><<<rows, kWarps * 32, smem, st>>>(
+          L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
+          stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13);
+    }
   }
   FMM_CUDA_TRY(cudaGetLastError());
 }
