@@ -572,8 +572,10 @@ __host__ __device__ constexpr size_t lane_smem_bytes() {
 }
 
 // one warp per CTA; warp b owns target tgt_list[b] and its sources src_of[off[b] .. off[b+1])
-template <int PMAX, class V>
-__global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_list, const int* __restrict__ off,
+// W warps per CTA share one target row (pairs strided over the warps), for launches of few
+// rows; the warps' accumulators are summed in warp order
+template <int PMAX, class V, int W = 1>
+__global__ void __launch_bounds__(32 * W) k_m2l_lane(const int* __restrict__ tgt_list, const int* __restrict__ off,
                                                  const int* __restrict__ src_of, double* __restrict__ local,
                                                  const double* __restrict__ multipole,
                                                  const double* __restrict__ tcen, const double* __restrict__ tbox,
@@ -585,12 +587,14 @@ __global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_lis
   constexpr int NH = hi(PMAX + 1, 0);
   constexpr bool F32 = sizeof(V) == 4;
   extern __shared__ double lane_smem[];
-  double* stage = lane_smem;                         // [2 (PMAX+1)][33]
+  constexpr size_t WSM = lane_smem_bytes<PMAX, V>() / sizeof(double);  // one warp's region
+  const int w = threadIdx.x >> 5;
+  double* stage = lane_smem + (size_t)w * WSM;       // [2 (PMAX+1)][33]
   double* acc = stage + 2 * (PMAX + 1) * 33;         // [2 NH]
   V* MsV = reinterpret_cast<V*>(acc + 2 * NH);       // rotated multipole [2 NH][32]
   double* Ms = reinterpret_cast<double*>(MsV);
   float* Msf = reinterpret_cast<float*>(MsV);
-  const int lane = threadIdx.x;
+  const int lane = threadIdx.x & 31;
   const int b = blockIdx.x;
   const int t = tgt_list[b];
   const double tc0 = tcen[3 * t], tc1 = tcen[3 * t + 1], tc2 = tcen[3 * t + 2];
@@ -605,7 +609,7 @@ __global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_lis
   bool fail = false;
   unsigned long long fl = 0;
   const int l0 = off[b], l1 = off[b + 1];
-  for (int lb = l0; lb < l1; lb += 32) {
+  for (int lb = l0 + 32 * w; lb < l1; lb += 32 * W) {
     Pair q;
     const int l = lb + lane;
     q.valid = l < l1;
@@ -703,7 +707,17 @@ __global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_lis
     __syncwarp();
   }
   double* dst = local + (int64_t)4 * NH * t;
-  for (int i = lane; i < 2 * NH; i += 32) dst[4 * (i >> 1) + (i & 1)] += acc[i];
+  if constexpr (W == 1) {
+    for (int i = lane; i < 2 * NH; i += 32) dst[4 * (i >> 1) + (i & 1)] += acc[i];
+  } else {
+    __syncthreads();
+    if (w == 0)
+      for (int i = lane; i < 2 * NH; i += 32) {
+        double v = acc[i];
+        for (int q = 1; q < W; ++q) v += acc[(size_t)q * WSM + i];
+        dst[4 * (i >> 1) + (i & 1)] += v;
+      }
+  }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     pmax = max(pmax, __shfl_xor_sync(kAll, pmax, o));
@@ -717,17 +731,35 @@ __global__ void __launch_bounds__(32) k_m2l_lane(const int* __restrict__ tgt_lis
   }
 }
 
+// launches of fewer M2L target rows than kWideM2LRowsPerSM per SM take kWideM2LWarps warps per row
+constexpr int kWideM2LWarps = 4;
+constexpr int kWideM2LRowsPerSM = 4;
+
 template <int PMAX, class V>
 void run_lane_v(DevTree& t, const DevTree& s, const DevLists& L, int em, double eps, int be, int* p_used, int* stats,
                 cudaStream_t st) {
   const size_t sm = lane_smem_bytes<PMAX, V>();
-  if (sm > 48 * 1024)
-    FMM_CUDA_TRY(cudaFuncSetAttribute(k_m2l_lane<PMAX, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   note_launch();
-  k_m2l_lane<PMAX, V><<<(int)L.n_m2l_targets, 32, sm, st>>>(
-      L.m2l_tgt.ptr, L.m2l_off.ptr, L.m2l_s.ptr, t.local.ptr, s.multipole.ptr, t.tcenter.ptr, t.tbox.ptr,
-      t.tradius.ptr, t.max_influence.ptr, s.scenter.ptr, em, eps, be, p_used, stats, stats + 1,
-      reinterpret_cast<unsigned long long*>(stats + 2));
+  int dev = 0, n_sm = 0;
+  FMM_CUDA_TRY(cudaGetDevice(&dev));
+  FMM_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  if (L.n_m2l_targets < (int64_t)kWideM2LRowsPerSM * n_sm) {
+    // few target rows (small problems, probe trees): kWideM2LWarps warps share each row
+    constexpr int WW = kWideM2LWarps;
+    FMM_CUDA_TRY(cudaFuncSetAttribute(k_m2l_lane<PMAX, V, WW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(WW * sm)));
+    k_m2l_lane<PMAX, V, WW><<<(int)L.n_m2l_targets, 32 * WW, WW * sm, st>>>(
+        L.m2l_tgt.ptr, L.m2l_off.ptr, L.m2l_s.ptr, t.local.ptr, s.multipole.ptr, t.tcenter.ptr, t.tbox.ptr,
+        t.tradius.ptr, t.max_influence.ptr, s.scenter.ptr, em, eps, be, p_used, stats, stats + 1,
+        reinterpret_cast<unsigned long long*>(stats + 2));
+  } else {
+    if (sm > 48 * 1024)
+      FMM_CUDA_TRY(cudaFuncSetAttribute(k_m2l_lane<PMAX, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_m2l_lane<PMAX, V><<<(int)L.n_m2l_targets, 32, sm, st>>>(
+        L.m2l_tgt.ptr, L.m2l_off.ptr, L.m2l_s.ptr, t.local.ptr, s.multipole.ptr, t.tcenter.ptr, t.tbox.ptr,
+        t.tradius.ptr, t.max_influence.ptr, s.scenter.ptr, em, eps, be, p_used, stats, stats + 1,
+        reinterpret_cast<unsigned long long*>(stats + 2));
+  }
   FMM_CUDA_TRY(cudaGetLastError());
 }
 
