@@ -109,6 +109,11 @@ CASES = [
                  interaction_list_method=fm.SelfTuning())),
     dict(name="clustered20k_p10", gen=lambda: clustered(20000, 2),
          kw=dict(expansion_order=10, leaf_size_source=64, multipole_acceptance=0.5)),
+    # ~4,000 target rows: the near field's 4-warp CTAs and the one-warp M2L rows (launches of fewer
+    # rows than 4 per SM take wider CTAs, which the smaller cases here exercise)
+    dict(name="uniform60k_p4_ls20", gen=lambda: uniform(60000, 31), kw=dict(expansion_order=4, leaf_size_source=20,
+                                                                           multipole_acceptance=0.5,
+                                                                           scalar_potential=True)),
     # the lane kernel's highest order
     dict(name="uniform6k_p12", gen=lambda: uniform(6000, 8), kw=dict(expansion_order=12, leaf_size_source=40,
                                                                      multipole_acceptance=0.5,
@@ -175,6 +180,26 @@ def test_vortex_lane_m2l_orders_match_oracle(ctx, p):
     for rows in (slice(4, 7), slice(7, 16)):
         scale = np.abs(ref["out"][:, rows]).max()
         np.testing.assert_allclose(out[:, rows], ref["out"][:, rows], rtol=0, atol=1e-10 * scale)
+
+
+def test_many_rows_vortex_and_mixed(ctx):
+    # ~4,000 target rows (the narrow near-field and M2L launches): FP64 vortex particles against the
+    # oracle, and the mixed point-source solve against the FP64 one
+    buf = ring(50000, 32)
+    og, oo = opt_pair(expansion_order=6, leaf_size_source=16, multipole_acceptance=0.5, hessian=True)
+    out, res = fm.solve_buffers(buf, L.FMM_POINT_VORTEX, og, ctx=ctx)
+    ref = O.fmm(buf, O.POINT_VORTEX, oo)
+    for rows in (slice(4, 7), slice(7, 16)):
+        scale = np.abs(ref["out"][:, rows]).max()
+        np.testing.assert_allclose(out[:, rows], ref["out"][:, rows], rtol=0, atol=1e-10 * scale)
+    pts = uniform(60000, 31)
+    outs = {}
+    for prec in ("f64", "mixed"):
+        og = fm.make_options(expansion_order=6, leaf_size_source=20, multipole_acceptance=0.5,
+                             error_tolerance=fm.PowerRelativeGradient(1e-6), scalar_potential=True, precision=prec)
+        outs[prec], res = fm.solve_buffers(pts, L.FMM_POINT_SOURCE, og, ctx=ctx)
+        assert res.n_m2l > 0
+    assert rel_l2(outs["mixed"][:, 4:7], outs["f64"][:, 4:7]) < 1e-5
 
 
 def test_mixed_vortex_matches_f64(ctx):
