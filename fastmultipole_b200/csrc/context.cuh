@@ -42,6 +42,10 @@ struct DevLists {
   int64_t n_m2l_targets = 0, n_dir_targets = 0;
   DevBuf<int> m2l_tgt, m2l_off;   // unique targets, offsets (n+1)
   DevBuf<int> dir_tgt, dir_off;
+  // near field of launches of few rows: rows cut into chunks of source leaves (row, leaf range,
+  // offset of the chunk's partial sums), their partial sums, and each row's chunk range
+  DevBuf<int4> p2p_chunks, p2p_rowtab;
+  DevBuf<double> p2p_part;
 };
 
 // Scratch shared by the stages of one solve.
@@ -93,7 +97,7 @@ void build_lists(DevLists& L, const DevTree& tt, const DevTree& stt, Scratch& sc
 
 // ---- p2p.cu ----
 // Near field over the direct list; accumulates into acc13 (sorted target order, 13 per body).
-void launch_p2p(const DevTree& tt, const DevTree& stt, const DevLists& L, double* acc13, int kind, bool ps,
+void launch_p2p(const DevTree& tt, const DevTree& stt, DevLists& L, double* acc13, int kind, bool ps,
                 bool gs, bool hs, int precision, cudaStream_t st);
 // sum over the direct list of n_target * n_source (atomically added to *out)
 void count_p2p_pairs(const DevTree& tt, const DevTree& stt, const DevLists& L, unsigned long long* out,

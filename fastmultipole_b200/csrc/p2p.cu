@@ -12,6 +12,8 @@
 // drop-in arithmetic; the MIXED variant moves every body relative to a nearby
 // centre in FP64, then evaluates the kernel in FP32 (rsqrt on the SFU),
 // summing blocks of sources in FP32 and the block partials in FP64.
+#include <climits>
+#include <vector>
 #include <algorithm>
 
 #include "context.cuh"
@@ -151,6 +153,8 @@ constexpr int kWarps = 4;
 // long rows (targets of a dual tree near many sources) would otherwise leave the SMs idle
 constexpr int kWideWarps = 16;
 constexpr int kWideRowsPerSM = 4;
+constexpr int kChunksPerSM = 8;  // chunks of the rows of such a launch, per SM
+constexpr double kChunkPairsMixed = 1e8, kChunkPairsF64 = 2e7;  // estimated pairs above which they are cut
 constexpr int kTPT = 2;
 constexpr unsigned kAll = 0xffffffffu;
 
@@ -406,7 +410,10 @@ __global__ void __launch_bounds__(W * 32) k_p2p(const int* __restrict__ tgt_list
                                                      const double* __restrict__ t_center,
                                                      const int* __restrict__ s_start, const int* __restrict__ s_count,
                                                      const double4* __restrict__ tpos, const double4* __restrict__ spos,
-                                                     const double4* __restrict__ sstr, double* __restrict__ acc13) {
+                                                     const double4* __restrict__ sstr, double* __restrict__ acc13,
+                                                     const int4* __restrict__ chunks, double* __restrict__ chunk_sums) {
+  // chunks (CTA path only; may be null): CTA b takes the source leaves [y, z) of row x and stores
+  // its sums (unscaled, not atomically) at chunk_sums + w + NA * (target index in the row) + channel
   constexpr int NB = batch_bodies<R, KIND>(), NV = Batch<KIND>::nv, NA = n_chan<KIND, GS, HS>();
   constexpr int NS = slots_per_body<R, KIND>();
   constexpr bool MIXED = sizeof(R) == 4;
@@ -420,11 +427,14 @@ __global__ void __launch_bounds__(W * 32) k_p2p(const int* __restrict__ tgt_list
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   R* B = reinterpret_cast<R*>(p2p_smem) + w * NS * NB;  // this warp's batch, plane v at B[v * NB]
   double* red = reinterpret_cast<double*>(p2p_smem + W * NS * NB * sizeof(R));  // [W][32 kTPT][NA]
-  const int row = RW ? blockIdx.x * W + w : blockIdx.x;
+  constexpr bool CH = !RW && W > kWarps;  // only the wide instances take chunks
+  const bool chunked = CH && chunks != nullptr;
+  const int4 ck = chunked ? chunks[blockIdx.x] : make_int4(0, 0, 0, 0);
+  const int row = RW ? blockIdx.x * W + w : (chunked ? ck.x : (int)blockIdx.x);
   if (RW && row >= n_rows) return;  // whole warps: no block barrier on the RW path
   constexpr int LS = RW ? 1 : W;  // stride of this warp's source leaves along the row
   const int t = tgt_list[row];
-  const int l0 = off[row], l1 = off[row + 1];
+  const int l0 = chunked ? ck.y : off[row], l1 = chunked ? ck.z : off[row + 1];
   const int ts = t_start[t], tc = t_count[t];
   const double ox = MIXED ? t_center[3 * t] : 0.0;
   const double oy = MIXED ? t_center[3 * t + 1] : 0.0;
@@ -658,6 +668,10 @@ __global__ void __launch_bounds__(W * 32) k_p2p(const int* __restrict__ tgt_list
       double v = 0;
 #pragma unroll
       for (int q = 0; q < W; ++q) v += red[(q * 32 * kTPT + i) * NA + a];
+      if (chunked) {
+        chunk_sums[ck.w + (int64_t)NA * (tile + i) + a] = v;
+        continue;
+      }
       if (KIND == FMM_POINT_SOURCE && a == 0 && !PS) continue;
       // atomic: under SelfTuning a non-leaf target branch and its own leaves can both own direct-list rows
       atomicAdd(acc13 + 13 * (int64_t)(ts + tile + i) + chan_row<KIND, GS>(a), v * kOneOver4Pi);
@@ -730,8 +744,29 @@ __global__ void __launch_bounds__(kP2PThreads) k_direct(const double4* __restric
   }
 }
 
+// Sums of the chunks of each row (rowtab[r] = first chunk, end) in chunk order, added to the
+// row's targets: the near field of launches whose rows were cut into chunks.
+template <int KIND, bool PS, bool GS, int NA>
+__global__ void k_p2p_chunk_sum(const int4* __restrict__ rowtab, const int4* __restrict__ chunks,
+                                const double* __restrict__ part, const int* __restrict__ tgt_list,
+                                const int* __restrict__ t_start, const int* __restrict__ t_count,
+                                double* __restrict__ acc13) {
+  const int r = blockIdx.x;
+  const int4 rt = rowtab[r];
+  const int t = tgt_list[r];
+  const int ts = t_start[t], tc = t_count[t];
+  for (int e = threadIdx.x; e < tc * NA; e += blockDim.x) {
+    const int i = e / NA, a = e - i * NA;
+    if (KIND == FMM_POINT_SOURCE && a == 0 && !PS) continue;
+    double v = 0.0;
+    for (int c = rt.x; c < rt.y; ++c) v += part[chunks[c].w + (int64_t)e];
+    // atomic: under SelfTuning a non-leaf target branch and its own leaves can both own rows
+    atomicAdd(acc13 + 13 * (int64_t)(ts + i) + chan_row<KIND, GS>(a), v * kOneOver4Pi);
+  }
+}
+
 template <class R, int KIND, bool PS, bool GS, bool HS>
-void run_p2p(const DevTree& tt, const DevTree& stt, const DevLists& L, double* acc13, cudaStream_t st) {
+void run_p2p(const DevTree& tt, const DevTree& stt, DevLists& L, double* acc13, cudaStream_t st) {
   if (L.n_dir_targets == 0) return;
   constexpr size_t smem = p2p_smem_bytes<R, KIND, GS, HS>();
   const int rows = (int)L.n_dir_targets;
@@ -744,25 +779,75 @@ void run_p2p(const DevTree& tt, const DevTree& stt, const DevLists& L, double* a
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_p2p<R, KIND, PS, GS, HS, true><<<(rows + kWarps - 1) / kWarps, kWarps * 32, smem, st>>>(
         L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
-        stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13);
+        stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13, nullptr,
+        nullptr);
   } else {
     int dev = 0, n_sm = 0;
     FMM_CUDA_TRY(cudaGetDevice(&dev));
     FMM_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-    if (rows < kWideRowsPerSM * n_sm) {
+    // estimated body pairs of the launch: chunking costs a host round trip and a second kernel,
+    // which only pays for launches of much work (the FP64 pairs cost ~5x the mixed ones)
+    const double est_pairs = (double)L.n_direct * ((double)stt.n_bodies / std::max<int64_t>(1, stt.n_leaves)) *
+                             ((double)tt.n_bodies / std::max<int64_t>(1, tt.n_leaves));
+    const bool chunk = est_pairs > (sizeof(R) == 4 ? kChunkPairsMixed : kChunkPairsF64);
+    if (rows < kWideRowsPerSM * n_sm && !chunk) {
       constexpr size_t smw = p2p_smem_bytes<R, KIND, GS, HS, kWideWarps>();
       FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2p<R, KIND, PS, GS, HS, false, kWideWarps>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw));
       k_p2p<R, KIND, PS, GS, HS, false, kWideWarps><<<rows, kWideWarps * 32, smw, st>>>(
           L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
-          stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13);
+          stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13, nullptr, nullptr);
+    } else if (rows < kWideRowsPerSM * n_sm) {
+      // few rows: cut them into chunks of about the same number of source leaves (some
+      // kChunksPerSM per SM over the launch), one wide CTA each; the chunks' partial sums are
+      // added in chunk order by k_p2p_chunk_sum
+      constexpr int NA = n_chan<KIND, GS, HS>();
+      std::vector<int> h_off(rows + 1), h_tgt(rows), h_cnt(tt.n_branches);
+      FMM_CUDA_TRY(cudaMemcpyAsync(h_off.data(), L.dir_off.ptr, (rows + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
+      FMM_CUDA_TRY(cudaMemcpyAsync(h_tgt.data(), L.dir_tgt.ptr, rows * sizeof(int), cudaMemcpyDeviceToHost, st));
+      FMM_CUDA_TRY(cudaMemcpyAsync(h_cnt.data(), tt.body_count.ptr, tt.n_branches * sizeof(int),
+                                   cudaMemcpyDeviceToHost, st));
+      FMM_CUDA_TRY(cudaStreamSynchronize(st));
+      const int64_t total = (int64_t)h_off[rows] - h_off[0], goal = (int64_t)kChunksPerSM * n_sm;
+      const int64_t per = std::max<int64_t>(2 * kWideWarps, (total + goal - 1) / goal);
+      std::vector<int4> ch, rt(rows);
+      int64_t out = 0;
+      for (int r = 0; r < rows; ++r) {
+        const int a = h_off[r], nl = h_off[r + 1] - a;
+        const int k = (int)std::max<int64_t>(1, (nl + per - 1) / per);
+        rt[r] = make_int4((int)ch.size(), (int)ch.size() + k, 0, 0);
+        const int64_t nt = h_cnt[h_tgt[r]];
+        for (int j = 0; j < k; ++j) {
+          ch.push_back(make_int4(r, a + (int)((int64_t)nl * j / k), a + (int)((int64_t)nl * (j + 1) / k), (int)out));
+          out += nt * NA;
+          FMM_CHECK(out < INT_MAX, FMM_ERR_MEMORY, "near-field chunk sums exceed the index range");
+        }
+      }
+      L.p2p_chunks.grow(ch.size());
+      L.p2p_rowtab.grow(rows);
+      L.p2p_part.grow((size_t)out + 1);
+      FMM_CUDA_TRY(cudaMemcpyAsync(L.p2p_chunks.ptr, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+      FMM_CUDA_TRY(cudaMemcpyAsync(L.p2p_rowtab.ptr, rt.data(), rt.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+      constexpr size_t smw = p2p_smem_bytes<R, KIND, GS, HS, kWideWarps>();
+      FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2p<R, KIND, PS, GS, HS, false, kWideWarps>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw));
+      k_p2p<R, KIND, PS, GS, HS, false, kWideWarps><<<(int)ch.size(), kWideWarps * 32, smw, st>>>(
+          L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
+          stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13, L.p2p_chunks.ptr,
+          L.p2p_part.ptr);
+      FMM_CUDA_TRY(cudaGetLastError());
+      note_launch();
+      k_p2p_chunk_sum<KIND, PS, GS, NA><<<rows, 256, 0, st>>>(L.p2p_rowtab.ptr, L.p2p_chunks.ptr, L.p2p_part.ptr,
+                                                               L.dir_tgt.ptr, tt.body_start.ptr, tt.body_count.ptr,
+                                                               acc13);
     } else {
       if (smem > 48 * 1024)
         FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2p<R, KIND, PS, GS, HS, false>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       k_p2p<R, KIND, PS, GS, HS, false><<<rows, kWarps * 32, smem, st>>>(
           L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
-          stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13);
+          stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13, nullptr,
+        nullptr);
     }
   }
   FMM_CUDA_TRY(cudaGetLastError());
@@ -800,7 +885,7 @@ void dispatch(int kind, bool ps, bool gs, bool hs, F& f) {
 struct P2PLaunch {
   const DevTree& tt;
   const DevTree& stt;
-  const DevLists& L;
+  DevLists& L;
   double* acc13;
   cudaStream_t st;
   template <class R, int K, bool PS, bool GS, bool HS>
@@ -844,7 +929,7 @@ void count_p2p_pairs(const DevTree& tt, const DevTree& stt, const DevLists& L, u
   FMM_CUDA_TRY(cudaGetLastError());
 }
 
-void launch_p2p(const DevTree& tt, const DevTree& stt, const DevLists& L, double* acc13, int kind, bool ps, bool gs,
+void launch_p2p(const DevTree& tt, const DevTree& stt, DevLists& L, double* acc13, int kind, bool ps, bool gs,
                 bool hs, int precision, cudaStream_t st) {
   P2PLaunch f{tt, stt, L, acc13, st};
   if (precision == FMM_PRECISION_MIXED)
