@@ -154,7 +154,7 @@ constexpr int kWarps = 4;
 constexpr int kWideWarps = 16;
 constexpr int kWideRowsPerSM = 4;
 constexpr int kChunksPerSM = 8;  // chunks of the rows of such a launch, per SM
-constexpr double kChunkPairsMixed = 1e8, kChunkPairsF64 = 2e7;  // estimated pairs above which they are cut
+constexpr double kChunkPairs = 1e8;  // estimated body pairs above which their rows are cut
 constexpr int kTPT = 2;
 constexpr unsigned kAll = 0xffffffffu;
 
@@ -786,10 +786,11 @@ void run_p2p(const DevTree& tt, const DevTree& stt, DevLists& L, double* acc13, 
     FMM_CUDA_TRY(cudaGetDevice(&dev));
     FMM_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
     // estimated body pairs of the launch: chunking costs a host round trip and a second kernel,
-    // which only pays for launches of much work (the FP64 pairs cost ~5x the mixed ones)
+    // which only pays for launches of much work (and the round trip holds back a serving
+    // worker's next launches)
     const double est_pairs = (double)L.n_direct * ((double)stt.n_bodies / std::max<int64_t>(1, stt.n_leaves)) *
                              ((double)tt.n_bodies / std::max<int64_t>(1, tt.n_leaves));
-    const bool chunk = est_pairs > (sizeof(R) == 4 ? kChunkPairsMixed : kChunkPairsF64);
+    const bool chunk = est_pairs > kChunkPairs;
     if (rows < kWideRowsPerSM * n_sm && !chunk) {
       constexpr size_t smw = p2p_smem_bytes<R, KIND, GS, HS, kWideWarps>();
       FMM_CUDA_TRY(cudaFuncSetAttribute(k_p2p<R, KIND, PS, GS, HS, false, kWideWarps>,
@@ -823,9 +824,11 @@ void run_p2p(const DevTree& tt, const DevTree& stt, DevLists& L, double* acc13, 
           FMM_CHECK(out < INT_MAX, FMM_ERR_MEMORY, "near-field chunk sums exceed the index range");
         }
       }
-      L.p2p_chunks.grow(ch.size());
-      L.p2p_rowtab.grow(rows);
-      L.p2p_part.grow((size_t)out + 1);
+      // floors of a few MB: regrowing frees device memory, which waits for the whole device (and
+      // for every other context's work on it)
+      L.p2p_chunks.grow(std::max<size_t>(ch.size(), 1 << 16));
+      L.p2p_rowtab.grow(std::max<size_t>(rows, 1 << 12));
+      L.p2p_part.grow(std::max<size_t>((size_t)out + 1, 1 << 19));
       FMM_CUDA_TRY(cudaMemcpyAsync(L.p2p_chunks.ptr, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
       FMM_CUDA_TRY(cudaMemcpyAsync(L.p2p_rowtab.ptr, rt.data(), rt.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
       constexpr size_t smw = p2p_smem_bytes<R, KIND, GS, HS, kWideWarps>();
