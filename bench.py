@@ -197,6 +197,21 @@ def cpu_baseline(w, n=None):
             "sample": f"{n:,} bodies of the same distribution, one fmm! of the C++ FP64 restatement, {dt:.2f} s"}
 
 
+def max_over_ranks(value, world, device="cpu"):
+    """The largest of the ranks' values (every rank passes its own and gets the max): the
+    slowest replica's time is the job's time."""
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(n_per_rank, world, ms_per_step):
+    """Whole-job throughput of world replicas of n_per_rank bodies each, at the slowest rank's time."""
+    return world * n_per_rank / (ms_per_step * 1e-3)
+
+
 def reference_arm(args, w, rank):
     if rank != 0:
         return
@@ -261,10 +276,7 @@ def gpu_arm(args, w, rank, world, local_rank):
             e1.synchronize()
             total += e0.elapsed_time(e1)
         barrier()
-        t = torch.tensor([total], dtype=torch.float64, device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item()) / steps  # ms per step, max over ranks
+        return max_over_ranks(total, world, dev) / steps  # ms per step, max over ranks
 
     opt_mixed = options(fm, w, "mixed")
     opt_f64 = options(fm, w, "f64")
@@ -329,7 +341,7 @@ def gpu_arm(args, w, rank, world, local_rank):
         roof = {"kernel": "k_m2l (FP64)", "bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": ach / fp64_peak, "traffic": None, "work": f"{st_mixed['m2l_flops']:.3e} algorithmic flop",
                 "peak_source": "nominal FP64 CUDA-core peak (half the FP32 rate)"}
-    value = world * n / (ms_mixed * 1e-3)
+    value = job_rate(n, world, ms_mixed)
     line = {
         "metric": METRIC,
         "value": value, "unit": "bodies/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -338,9 +350,9 @@ def gpu_arm(args, w, rank, world, local_rank):
         "config": {"workload": w["workload"], "n_bodies": n, "precision": "mixed", "parallelism": f"replicas x{world}",
                    "l2": "256 MB buffer written between timed steps"},
         "rel_err_vs_direct": errs["mixed"], "f64_rel_err_vs_direct": errs["f64"],
-        "f64_value": world * n / (ms_f64 * 1e-3), "f64_ms_per_step": ms_f64,
+        "f64_value": job_rate(n, world, ms_f64), "f64_ms_per_step": ms_f64,
         "speedup_mixed_vs_f64": ms_f64 / ms_mixed,
-        "e2e": {"value": world * n / (ms_e2e * 1e-3), "unit": "bodies/s", "ms_per_step": ms_e2e,
+        "e2e": {"value": job_rate(n, world, ms_e2e), "unit": "bodies/s", "ms_per_step": ms_e2e,
                 "h2d_bytes_per_step": int(buf.nbytes), "d2h_bytes_per_step": int(n * 16 * 8)},
         "gpu_launches": int(launches) * args.steps,
         "stages_ms": stages, "f64_stages_ms": {"nearfield": st_f64["t_nearfield_ms"],
