@@ -202,6 +202,24 @@ def test_many_rows_vortex_and_mixed(ctx):
     assert rel_l2(outs["mixed"][:, 4:7], outs["f64"][:, 4:7]) < 1e-5
 
 
+def test_chunked_near_field_probes_match_oracle(ctx):
+    # 10,000 probes around 200,000 sources: 456 target rows, a few of them with most of the pairs,
+    # so the near field cuts the rows into chunks of source leaves (summed in chunk order)
+    rng = np.random.default_rng(4)
+    buf = uniform(200000, 41)
+    probes = np.ascontiguousarray(-0.5 + 2.0 * rng.random((10000, 3)))
+    og, oo = opt_pair(expansion_order=8, leaf_size_source=50, multipole_acceptance=0.5, scalar_potential=True)
+    out, res = fm.solve_buffers(buf, L.FMM_POINT_SOURCE, og, target_pos=probes, ctx=ctx)
+    ref = O.fmm(buf, O.POINT_SOURCE, oo, target_pos=probes)
+    rows = slice(3, 7)
+    scale = np.abs(ref["out"][:, rows]).max()
+    np.testing.assert_allclose(out[:, rows], ref["out"][:, rows], rtol=0, atol=1e-10 * scale)
+    omx = fm.make_options(expansion_order=8, leaf_size_source=50, multipole_acceptance=0.5, scalar_potential=True,
+                          precision="mixed")
+    mx, _ = fm.solve_buffers(buf, L.FMM_POINT_SOURCE, omx, target_pos=probes, ctx=ctx)
+    assert rel_l2(mx[:, 4:7], out[:, 4:7]) < 1e-5
+
+
 def test_mixed_vortex_matches_f64(ctx):
     # FP32 near field (batch sums promoted to FP64): relative L2 deviation from the FP64 solve below 1e-5
     buf = ring(20000, 7)
