@@ -651,6 +651,7 @@ int fmm_solve(fmm_ctx* c, const fmm_target_system* target, const fmm_source_syst
     FMM_CHECK(target != nullptr, FMM_ERR_ARGUMENT, "target system is NULL (it carries the output buffer)");
     const bool self = target->positions == nullptr;  // fmm!(system): the sources are the targets
     FMM_CHECK(self || target->stride >= 3, FMM_ERR_ARGUMENT, "target stride must be >= 3");
+    FMM_CHECK(self || target->n_bodies >= 0, FMM_ERR_ARGUMENT, "negative target n_bodies");
     FMM_CUDA_TRY(cudaSetDevice(c->device));
     if (result) std::memset(result, 0, sizeof(*result));
     SolveIn in;
@@ -714,6 +715,7 @@ int fmm_solve_multi(fmm_ctx* c, const fmm_target_system* target, const fmm_sourc
     FMM_CHECK(target->stride >= 3, FMM_ERR_ARGUMENT, "target stride must be >= 3");
     FMM_CHECK(opt != nullptr, FMM_ERR_ARGUMENT, "options are NULL");
     const int64_t nt = target->n_bodies;
+    FMM_CHECK(nt >= 0, FMM_ERR_ARGUMENT, "negative target n_bodies");
     FMM_CHECK(nt == 0 || target->out, FMM_ERR_ARGUMENT, "target out buffer is NULL");
     FMM_CUDA_TRY(cudaSetDevice(c->device));
     fmm_result total;
@@ -790,6 +792,7 @@ int fmm_vjp(fmm_ctx* c, const fmm_target_system* target, const fmm_source_system
     FMM_CHECK(target != nullptr, FMM_ERR_ARGUMENT, "target system is NULL (it carries the forward output)");
     const bool self = target->positions == nullptr;
     FMM_CHECK(self || target->stride >= 3, FMM_ERR_ARGUMENT, "target stride must be >= 3");
+    FMM_CHECK(self || target->n_bodies >= 0, FMM_ERR_ARGUMENT, "negative target n_bodies");
     const int64_t ns = source->n_bodies, nt = self ? source->n_bodies : target->n_bodies;
     FMM_CHECK(ns > 0 && nt > 0, FMM_ERR_ARGUMENT, "fmm_vjp needs sources and targets");
     FMM_CHECK(target->out && d_out && d_strength && d_source_position, FMM_ERR_ARGUMENT,
@@ -877,6 +880,7 @@ int fmm_direct(fmm_ctx* c, const fmm_target_system* target, const fmm_source_sys
     const bool self = target->positions == nullptr;
     const int64_t nt = self ? source->n_bodies : target->n_bodies;
     FMM_CHECK(self || target->stride >= 3, FMM_ERR_ARGUMENT, "target stride must be >= 3");
+    FMM_CHECK(nt >= 0, FMM_ERR_ARGUMENT, "negative target n_bodies");
     FMM_CHECK(nt == 0 || target->out, FMM_ERR_ARGUMENT, "target out buffer is NULL");
     FMM_CHECK(precision == FMM_PRECISION_F64 || precision == FMM_PRECISION_MIXED, FMM_ERR_ARGUMENT,
               "unknown precision");

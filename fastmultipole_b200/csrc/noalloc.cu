@@ -25,23 +25,37 @@ namespace {
 constexpr int64_t kNoAllocMaxBodies = 32768;
 constexpr int64_t kNoAllocDoubles = kNoAllocMaxBodies * (4 + 4 + 4 + 13);
 
-__device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
 // In host code `g_noalloc_scratch` names a host-side stand-in, not device memory;
-// its device address is looked up once per device with that device current.
-struct ScratchAddr {
-  std::once_flag once;
-  double* ptr = nullptr;
-  cudaError_t err = cudaSuccess;
-};
-ScratchAddr g_addr[64];
+// its device address is looked up with that device current.  Only a successful
+// lookup is kept, so a failed first attempt (a pending error, a call made during
+// a capture) is retried by the next call instead of disabling the device.
+std::mutex g_addr_mutex;
+double* g_addr[64] = {};
 
 double* scratch_for(int device, cudaError_t& err) {
-  ScratchAddr& a = g_addr[device];
-  std::call_once(a.once, [&] { a.err = cudaGetSymbolAddress((void**)&a.ptr, g_noalloc_scratch); });
-  err = a.err;
-  return a.err == cudaSuccess ? a.ptr : nullptr;
+  std::lock_guard<std::mutex> lock(g_addr_mutex);
+  err = cudaSuccess;
+  if (!g_addr[device]) {
+    double* ptr = nullptr;
+    err = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
+    if (err != cudaSuccess) return nullptr;
+    g_addr[device] = ptr;
+  }
+  return g_addr[device];
 }
+
+// The caller's current device is restored on every return.
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 
 __global__ void k_unpack_na(const double* __restrict__ buf, int64_t n, int64_t stride, int ns, int has_r,
                             double4* __restrict__ pos, double4* __restrict__ str) {
@@ -86,6 +100,7 @@ extern "C" FMM_API int fmm_direct_noalloc(int device, void* cuda_stream, const f
   if (source->data_per_body < 4 + source->kind || source->n_bodies < 0) return FMM_ERR_ARGUMENT;
   if (precision != FMM_PRECISION_F64 && precision != FMM_PRECISION_MIXED) return FMM_ERR_ARGUMENT;
   const bool self = target->positions == nullptr;
+  if (!self && target->n_bodies < 0) return FMM_ERR_ARGUMENT;
   const int64_t nt = self ? source->n_bodies : target->n_bodies;
   const int64_t ns = source->n_bodies;
   // device-resident inputs and output only: staging host memory would need device memory
@@ -94,6 +109,7 @@ extern "C" FMM_API int fmm_direct_noalloc(int device, void* cuda_stream, const f
   if ((ns > 0 && !source->buffer) || (nt > 0 && !target->out)) return FMM_ERR_ARGUMENT;
   if (ns > kNoAllocMaxBodies || nt > kNoAllocMaxBodies) return FMM_ERR_MEMORY;  // beyond the static scratch
   if (device < 0 || device >= 64) return FMM_ERR_ARGUMENT;
+  DeviceGuard restore;
   if (cudaSetDevice(device) != cudaSuccess) return FMM_ERR_NO_DEVICE;
   if (nt == 0) return FMM_OK;
   cudaError_t err;

@@ -236,8 +236,10 @@ FMM_API int fmm_serve_stop(fmm_ctx* ctx);
  * The work is queued on `cuda_stream` (NULL = legacy default stream) and the
  * call returns without synchronising; target->out is valid in stream order.
  * The first call on a device looks up the array's device address, so make
- * that first call before any stream capture.  Calls share the array: calls
- * that overlap on the GPU (other streams or host threads) race on it. */
+ * that first call before any stream capture (a failed lookup is retried by the
+ * next call).  Calls share the array: calls that overlap on the GPU (other
+ * streams or host threads) race on it.  The caller's current device is
+ * restored before the call returns. */
 FMM_API int fmm_direct_noalloc(int device, void* cuda_stream, const fmm_target_system* target,
                                const fmm_source_system* source, int scalar_potential, int gradient, int hessian,
                                int precision);

@@ -6,15 +6,17 @@ fixture holds, per case, the coefficient vectors in the reference's
 "full" ordering (n = 0..p, m = -n..n) as [re, im] pairs, plus the scalar
 parameters of the case as they appear in the test file.
 
-Usage:  python tests/golden/make_golden.py [path/to/FastMultipole.jl]
-(the default path is the read-only reference checkout of this build host).
+Usage:  python tests/golden/make_golden.py path/to/FastMultipole.jl
+(the path of a FastMultipole.jl checkout is required).
 """
 import json
 import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py path/to/FastMultipole.jl")
+REF = sys.argv[1]
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_vectors.json")
 
 NUM = r"[-+]?(?:\d+\.?\d*|\.\d+)(?:[eE][-+]?\d+)?"
