@@ -381,8 +381,9 @@ def solve_multi_buffers(sources, opt, target_pos, ctx=None):
 def vjp_buffers(source_buf, kind, opt, d_out, target_pos=None, ctx=None):
     """Gradients of a loss through fmm! on raw buffers (fmm_vjp).
 
-    ``d_out`` (Nt, 16) holds dL/d(target buffer): column 3 (phi) for point sources,
-    columns 4..6 (velocity) for vortex particles.  Returns ``(out, d_strength,
+    ``d_out`` (Nt, 16) holds dL/d(target buffer): columns 0..2 (the echoed target
+    positions) and column 3 (phi) for point sources, columns 0..2 and 4..6 (velocity) for
+    vortex particles; a non-zero value in any other column is rejected.  Returns ``(out, d_strength,
     d_source_position, d_target_position, fmm_result)``: the forward target buffer,
     dL/dstrength (N,) or (N, 3), dL/dx (N, 3) and, for separate targets, dL/dy
     (Nt, 3) (None when the sources are the targets)."""

@@ -64,6 +64,18 @@ __global__ void k_unsort_gradnorm(const double* __restrict__ acc13, const int* _
   }
 }
 
+// rows of the target buffer whose cotangents the adjoint does not propagate: the gradient and
+// Hessian of point sources (they would need dipole sources), the potential row and the
+// velocity gradient of vortex particles
+__device__ __host__ inline bool vjp_unsupported_row(int kind, int r) {
+  return kind == FMM_POINT_SOURCE ? r >= 4 : (r == 3 || r >= 7);
+}
+
+__global__ void k_check_cotangents(int64_t n, int kind, const double* __restrict__ dout16, int* __restrict__ flag) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 16 * n; i += (int64_t)gridDim.x * blockDim.x)
+    if (vjp_unsupported_row(kind, (int)(i % 16)) && dout16[i] != 0.0) atomicExch(flag, 1);
+}
+
 int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); }
 
 // out += in on rows 4..16 of the target buffer (rows 1..3 are the positions)
@@ -108,7 +120,7 @@ __global__ void k_vjp_sources(int64_t n, int kind, const double* __restrict__ sr
       dstr[i] = a[3];
       for (int k = 0; k < 3; ++k) {
         double v = -q * a[4 + k];
-        if (fwd16) v -= dout16[16 * i + 3] * fwd16[16 * i + 4 + k];
+        if (fwd16) v += dout16[16 * i + k] - dout16[16 * i + 3] * fwd16[16 * i + 4 + k];
         dpos[3 * i + k] = v;
       }
     } else {
@@ -117,24 +129,27 @@ __global__ void k_vjp_sources(int64_t n, int kind, const double* __restrict__ sr
       for (int k = 0; k < 3; ++k) {
         double v = 0.0;
         for (int c = 0; c < 3; ++c) v += G[c] * a[7 + c + 3 * k];
-        if (fwd16)
+        if (fwd16) {
+          v += dout16[16 * i + k];
           for (int c = 0; c < 3; ++c) v += dout16[16 * i + 4 + c] * fwd16[16 * i + 7 + c + 3 * k];
+        }
         dpos[3 * i + k] = v;
       }
     }
   }
 }
 
-// dL/dy at a separate target system, from the forward solve
+// dL/dy at a separate target system, from the forward solve (rows 1..3 of the target
+// buffer are the target positions themselves: their cotangents pass through)
 __global__ void k_vjp_targets(int64_t n, int kind, const double* __restrict__ fwd16, const double* __restrict__ dout16,
                               double* __restrict__ dtp) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double* f = fwd16 + 16 * i;
     const double* w = dout16 + 16 * i;
     for (int k = 0; k < 3; ++k) {
-      double v = 0.0;
+      double v = w[k];
       if (kind == FMM_POINT_SOURCE)
-        v = -w[3] * f[4 + k];
+        v -= w[3] * f[4 + k];
       else
         for (int c = 0; c < 3; ++c) v += w[4 + c] * f[7 + c + 3 * k];
       dtp[3 * i + k] = v;
@@ -822,6 +837,21 @@ int fmm_vjp(fmm_ctx* c, const fmm_target_system* target, const fmm_source_system
       in.t_stride = target->stride;
     }
     const double* dout = stage(c, c->stage_d, d_out, 16 * (size_t)nt, mem);
+    {
+      // a cotangent the adjoint would ignore is an error, not a silently wrong gradient
+      c->sc.flag.grow(1);
+      FMM_CUDA_TRY(cudaMemsetAsync(c->sc.flag.ptr, 0, sizeof(int), c->stream));
+      note_launch();
+      k_check_cotangents<<<grid_for(16 * nt), 256, 0, c->stream>>>(nt, kind, dout, c->sc.flag.ptr);
+      FMM_CUDA_TRY(cudaGetLastError());
+      int bad = 0;
+      FMM_CUDA_TRY(cudaMemcpyAsync(&bad, c->sc.flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+      FMM_CHECK(!bad, FMM_ERR_ARGUMENT,
+                kind == FMM_POINT_SOURCE
+                    ? "fmm_vjp: point sources propagate cotangents of rows 1..4 (positions, potential) only"
+                    : "fmm_vjp: vortex particles propagate cotangents of rows 1..3 and 5..7 (positions, velocity) only");
+    }
     c->out16.grow(16 * (size_t)nt);
     run_fmm(c, c->main, in, of, c->out16.ptr, result, false, c->stream, c->sc, c->stats);
     // adjoint solve: sources at the targets with the cotangents as strengths, targets at the sources
@@ -972,19 +1002,10 @@ int fmm_get_lists(fmm_ctx* c, int32_t* m2l, int64_t* n_m2l, int32_t* direct, int
     DevLists& L = c->main.lists;
     if (n_m2l) *n_m2l = L.n_m2l;
     if (n_direct) *n_direct = L.n_direct;
-    FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    auto pairs = [&](const DevBuf<int>& t, const DevBuf<int>& s, int64_t n, int32_t* dst) {
-      if (!dst || n == 0) return;
-      std::vector<int> ht(n), hs(n);
-      FMM_CUDA_TRY(cudaMemcpy(ht.data(), t.ptr, n * sizeof(int), cudaMemcpyDeviceToHost));
-      FMM_CUDA_TRY(cudaMemcpy(hs.data(), s.ptr, n * sizeof(int), cudaMemcpyDeviceToHost));
-      for (int64_t i = 0; i < n; ++i) {
-        dst[2 * i] = ht[i];
-        dst[2 * i + 1] = hs[i];
-      }
-    };
-    pairs(L.m2l_t, L.m2l_s, L.n_m2l, m2l);
-    pairs(L.dir_t, L.dir_s, L.n_direct, direct);
+    if (m2l || direct) {
+      FMM_CUDA_TRY(cudaSetDevice(c->device));
+      export_lists_reference_order(L, c->main.target(), c->main.source(), c->sc, c->stream, m2l, direct);
+    }
     return FMM_OK;
   } catch (const Error& e) {
     return fail(c, e);

@@ -46,6 +46,11 @@ struct DevLists {
   // offset of the chunk's partial sums), their partial sums, and each row's chunk range
   DevBuf<int4> p2p_chunks, p2p_rowtab;
   DevBuf<double> p2p_part;
+  // the traversal's rule (for the reference-order export)
+  double rule_mac = 0.5;
+  int64_t rule_ls = 1;
+  int rule_method = 0;
+  bool rule_ff = true, rule_nf = true, rule_si = true;
 };
 
 // Scratch shared by the stages of one solve.
@@ -94,6 +99,11 @@ void branch_max_influence(DevTree& t, const double* gnorm_orig, cudaStream_t st)
 void build_lists(DevLists& L, const DevTree& tt, const DevTree& stt, Scratch& sc, cudaStream_t st,
                  int64_t leaf_size_source, double mac, bool ff, bool nf, bool si, int method,
                  bool m2l_by_separation);
+// The lists of the last build in the reference's order: target rows ascending and, inside a
+// row, the order in which the depth-first recursion emitted the pairs (host arrays of
+// (target, source) pairs, n_m2l / n_direct of them; either may be null).
+void export_lists_reference_order(const DevLists& L, const DevTree& tt, const DevTree& stt, Scratch& sc,
+                                  cudaStream_t st, int32_t* m2l, int32_t* direct);
 
 // ---- p2p.cu ----
 // Near field over the direct list; accumulates into acc13 (sorted target order, 13 per body).

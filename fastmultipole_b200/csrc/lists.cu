@@ -596,6 +596,150 @@ void build_lists(DevLists& L, const DevTree& tt, const DevTree& stt, Scratch& sc
   L.n_m2l = n_m2l;
   L.n_dir_targets = rows[0];
   L.n_m2l_targets = rows[1];
+  L.rule_mac = mac;
+  L.rule_ls = leaf_size_source;
+  L.rule_method = method;
+  L.rule_ff = ff;
+  L.rule_nf = nf;
+  L.rule_si = si;
+}
+
+namespace {
+
+constexpr int kMaxDepth = 24;      // ancestor chain of a branch (the octant key allows 21 levels)
+constexpr int kStepsPerWord = 21;  // 3 bits per step, 63 bits per key word
+
+// Depth-first rank of every pair: the reference's recursion (src/interaction_list.jl:3-166)
+// reaches (t, s) from (root, root) by one split per step, each into the child that is an
+// ancestor of t (target split) or of s (source split); the side is the rule's decision at
+// that pair.  The child ordinals along the way (3 bits each, first step most significant)
+// order the pairs as the recursion emits them (no emitted pair's path is a prefix of
+// another's, so zero padding keeps the order).  An inconsistent path raises the flag.
+__global__ void k_dfs_keys(const int* __restrict__ lt, const int* __restrict__ ls, int n, TreeRef T, TreeRef S,
+                           const int* __restrict__ parent_t, const int* __restrict__ parent_s, Rule R,
+                           unsigned long long* __restrict__ khi, unsigned long long* __restrict__ klo,
+                           int* __restrict__ perm, int* __restrict__ flag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int ct[kMaxDepth], cs[kMaxDepth];
+    int nt = 0, ns = 0;
+    for (int a = lt[i]; a >= 0 && nt < kMaxDepth; a = parent_t[a]) ct[nt++] = a;
+    for (int b = ls[i]; b >= 0 && ns < kMaxDepth; b = parent_s[b]) cs[ns++] = b;
+    unsigned long long hi = 0, lo = 0;
+    bool bad = ct[nt - 1] != 0 || cs[ns - 1] != 0;
+    int it = nt - 1, is = ns - 1, step = 0;
+    while (!bad && (it > 0 || is > 0)) {
+      int nn, c0;
+      const int act = decide(T, ct[it], S, cs[is], R, nn, c0);
+      int ord;
+      if (act == A_SPLIT_T && it > 0) {
+        ord = ct[it - 1] - c0;
+        --it;
+      } else if (act == A_SPLIT_S && is > 0) {
+        ord = cs[is - 1] - c0;
+        --is;
+      } else {
+        bad = true;
+        break;
+      }
+      if (ord < 0 || ord >= nn || ord > 7 || step >= 2 * kStepsPerWord) {
+        bad = true;
+        break;
+      }
+      if (step < kStepsPerWord)
+        hi |= (unsigned long long)ord << (3 * (kStepsPerWord - 1 - step));
+      else
+        lo |= (unsigned long long)ord << (3 * (2 * kStepsPerWord - 1 - step));
+      ++step;
+    }
+    if (bad) atomicExch(flag, 1);
+    khi[i] = hi;
+    klo[i] = lo;
+    perm[i] = i;
+  }
+}
+
+__global__ void k_permute_u64(const unsigned long long* __restrict__ in, const int* __restrict__ perm, int n,
+                              unsigned long long* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = in[perm[i]];
+}
+
+__global__ void k_gather_pairs(const int* __restrict__ lt, const int* __restrict__ ls, const int* __restrict__ perm,
+                               int n, int2* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int j = perm[i];
+    out[i] = make_int2(lt[j], ls[j]);
+  }
+}
+
+}  // namespace
+
+void export_lists_reference_order(const DevLists& L, const DevTree& tt, const DevTree& stt, Scratch& sc,
+                                  cudaStream_t st, int32_t* m2l, int32_t* direct) {
+  const int nt = (int)tt.n_branches, ns = (int)stt.n_branches;
+  sc.node_geo_t.grow((size_t)nt);
+  sc.node_info_t.grow((size_t)nt);
+  sc.node_geo_s.grow((size_t)ns);
+  sc.node_info_s.grow((size_t)ns);
+  note_launch();
+  k_pack_nodes<<<blocks_for(nt, 256), 256, 0, st>>>(nt, tt.tcenter.ptr, tt.tradius.ptr, tt.n_children.ptr,
+                                                     tt.child_start.ptr, tt.body_count.ptr, sc.node_geo_t.ptr,
+                                                     sc.node_info_t.ptr);
+  note_launch();
+  k_pack_nodes<<<blocks_for(ns, 256), 256, 0, st>>>(ns, stt.scenter.ptr, stt.sradius.ptr, stt.n_children.ptr,
+                                                     stt.child_start.ptr, stt.body_count.ptr, sc.node_geo_s.ptr,
+                                                     sc.node_info_s.ptr);
+  FMM_CUDA_TRY(cudaGetLastError());
+  const TreeRef T{sc.node_geo_t.ptr, sc.node_info_t.ptr};
+  const TreeRef S{sc.node_geo_s.ptr, sc.node_info_s.ptr};
+  const Rule R{L.rule_mac, L.rule_ls, L.rule_method, L.rule_ff, L.rule_nf, L.rule_si};
+  struct One {
+    const DevBuf<int>*t, *s, *off;
+    int64_t n, rows;
+    int32_t* dst;
+  } lists[2] = {{&L.m2l_t, &L.m2l_s, &L.m2l_off, L.n_m2l, L.n_m2l_targets, m2l},
+                {&L.dir_t, &L.dir_s, &L.dir_off, L.n_direct, L.n_dir_targets, direct}};
+  sc.flag.grow(1);
+  for (const One& q : lists) {
+    if (!q.dst || q.n == 0) continue;
+    const int n = (int)q.n, rows = (int)q.rows;
+    sc.keys_a.grow(2 * (size_t)n);
+    sc.keys_b.grow(2 * (size_t)n);
+    sc.vals_a.grow((size_t)n);
+    sc.vals_b.grow((size_t)n);
+    unsigned long long *hi = sc.keys_a.ptr, *lo = sc.keys_a.ptr + n, *k1 = sc.keys_b.ptr, *k2 = sc.keys_b.ptr + n;
+    FMM_CUDA_TRY(cudaMemsetAsync(sc.flag.ptr, 0, sizeof(int), st));
+    note_launch();
+    k_dfs_keys<<<blocks_for(n, 256), 256, 0, st>>>(q.t->ptr, q.s->ptr, n, T, S, tt.parent.ptr, stt.parent.ptr, R, hi,
+                                                  lo, sc.vals_a.ptr, sc.flag.ptr);
+    FMM_CUDA_TRY(cudaGetLastError());
+    // lexicographic (hi, lo) inside every row: stable sort by lo, then stable sort by hi
+    const int* beg = q.off->ptr;
+    const int* end = q.off->ptr + 1;
+    size_t tb = 0, tb2 = 0;
+    FMM_CUDA_TRY(cub::DeviceSegmentedSort::StableSortPairs(nullptr, tb, lo, k1, sc.vals_a.ptr, sc.vals_b.ptr, n, rows,
+                                                           beg, end, st));
+    FMM_CUDA_TRY(cub::DeviceSegmentedSort::StableSortPairs(nullptr, tb2, hi, k2, sc.vals_b.ptr, sc.vals_a.ptr, n,
+                                                           rows, beg, end, st));
+    sc.cub.grow(std::max(tb, tb2));
+    note_launch();
+    FMM_CUDA_TRY(cub::DeviceSegmentedSort::StableSortPairs(sc.cub.ptr, tb, lo, k1, sc.vals_a.ptr, sc.vals_b.ptr, n,
+                                                           rows, beg, end, st));
+    // the second pass needs the hi keys in the order of the first: gather them
+    note_launch();
+    k_permute_u64<<<blocks_for(n, 256), 256, 0, st>>>(hi, sc.vals_b.ptr, n, lo);
+    note_launch();
+    FMM_CUDA_TRY(cub::DeviceSegmentedSort::StableSortPairs(sc.cub.ptr, tb2, lo, k2, sc.vals_b.ptr, sc.vals_a.ptr, n,
+                                                           rows, beg, end, st));
+    sc.front_a.grow((size_t)n);
+    note_launch();
+    k_gather_pairs<<<blocks_for(n, 256), 256, 0, st>>>(q.t->ptr, q.s->ptr, sc.vals_a.ptr, n, sc.front_a.ptr);
+    FMM_CUDA_TRY(cudaGetLastError());
+    int bad = 0;
+    FMM_CUDA_TRY(cudaMemcpyAsync(&bad, sc.flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FMM_CUDA_TRY(cudaMemcpyAsync(q.dst, sc.front_a.ptr, (size_t)n * sizeof(int2), cudaMemcpyDeviceToHost, st));
+    FMM_CUDA_TRY(cudaStreamSynchronize(st));
+    FMM_CHECK(!bad, FMM_ERR_STATE, "a list pair is not reachable by the traversal rule (reference-order export)");
+  }
 }
 
 }  // namespace fmmb

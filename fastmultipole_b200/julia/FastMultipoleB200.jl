@@ -19,6 +19,7 @@ names so existing overloads apply unchanged):
 module FastMultipoleB200
 
 import FastMultipole
+import ChainRulesCore
 import FastMultipole: source_system_to_buffer!, data_per_body, get_position, strength_dims, get_n_bodies,
                       buffer_to_target_system!, has_vector_potential, DerivativesSwitch, Point, Source, Vortex,
                       PowerAbsoluteGradient, PowerRelativeGradient, RotatedCoefficientsAbsoluteGradient,
@@ -242,6 +243,96 @@ function vjp(system, cotangent; targets=nothing, expansion_order=5, leaf_size=20
                     self_eval ? Ptr{Cdouble}(C_NULL) : pointer(d_tpos), res))
     end
     return vortex ? d_str : vec(d_str), d_pos, self_eval ? nothing : d_tpos
+end
+
+# ---- differentiable form (the reference is differentiated with ForwardDiff/ReverseDiff
+# through its Julia code, README.md:19; here the gradient is the adjoint FMM) ----
+
+function _options(; expansion_order=5, leaf_size_source=20, multipole_acceptance=0.4, error_tolerance=nothing,
+                  shrink_recenter=true, interaction_list_method=SelfTuningTreeStop(), scalar_potential=true,
+                  gradient=true, hessian=false, precision=:f64)
+    em, eps, be = error_code(error_tolerance)
+    return FmmOptions(expansion_order, leaf_size_source, 0, multipole_acceptance, em, eps, be, shrink_recenter,
+                      list_code(interaction_list_method), 1, 1, 1, 1, 1, 1, scalar_potential, gradient, hessian,
+                      precision == :mixed ? 1 : 0)
+end
+
+"""
+    fmm_buffer(source_buffer, target_positions, kind; kwargs...) -> 16 x n_t matrix
+
+`fmm!` as a pure function of arrays: `source_buffer` is the d x n_s buffer that
+`source_system_to_buffer!` fills (rows 1:3 position, 4 radius, 5:d strength),
+`target_positions` a 3 x n_t matrix or `nothing` (the sources are the targets),
+`kind` `:source` (Laplace point sources) or `:vortex`.  Returns the target buffer
+(rows 1:3 positions, 4 potential, 5:7 gradient / velocity, 8:16 Hessian / velocity
+gradient).  Keyword arguments as `fmm!`.  Differentiable through the
+`ChainRulesCore.rrule` below (and so with any ChainRules-aware AD, or ReverseDiff
+via `ReverseDiff.@grad_from_chainrules fmm_buffer(x::TrackedArray, y, k; kw...)`).
+"""
+function fmm_buffer(source_buffer::AbstractMatrix, target_positions, kind::Symbol; kwargs...)
+    buf = Matrix{Float64}(source_buffer)
+    n_s = size(buf, 2)
+    self_eval = target_positions === nothing
+    pos = self_eval ? buf : Matrix{Float64}(target_positions)
+    n_t = self_eval ? n_s : size(pos, 2)
+    out = zeros(Float64, 16, n_t)
+    opt = _options(; kwargs...)
+    res = FmmResult()
+    GC.@preserve buf pos out begin
+        src = FmmSourceSystem(kind === :vortex ? Cint(3) : Cint(1), n_s, size(buf, 1), pointer(buf), 0)
+        tgt = FmmTargetSystem(n_t, self_eval ? Ptr{Cdouble}(C_NULL) : pointer(pos), self_eval ? 0 : size(pos, 1),
+                              pointer(out), 0)
+        check(ccall((:fmm_solve, libfmm), Cint,
+                    (Ptr{Cvoid}, Ref{FmmTargetSystem}, Ref{FmmSourceSystem}, Ref{FmmOptions}, Ref{FmmResult}),
+                    context(), tgt, src, opt, res))
+    end
+    return out
+end
+
+"""
+ChainRulesCore.rrule of `fmm_buffer`: the pullback runs `fmm_vjp` (forward solve plus
+the adjoint solve whose sources sit at the targets with the cotangents as strengths).
+Cotangents are read from rows 1:3 (positions) and 4 (potential) for point sources,
+rows 1:3 and 5:7 (velocity) for vortex particles; a non-zero cotangent on another
+row is an error (libfmmb200 status 1).  Tangents: the source buffer (positions and
+strengths; the radius row gets zero) and the target positions; none for `kind`.
+Not executed in this repository: Julia is not installed on the build image, so the
+adjoint it calls is tested through the same C ABI from Python.
+"""
+function ChainRulesCore.rrule(::typeof(fmm_buffer), source_buffer::AbstractMatrix, target_positions, kind::Symbol;
+                              kwargs...)
+    out = fmm_buffer(source_buffer, target_positions, kind; kwargs...)
+    function fmm_buffer_pullback(Δout)
+        Δ = Matrix{Float64}(ChainRulesCore.unthunk(Δout))
+        buf = Matrix{Float64}(source_buffer)
+        n_s = size(buf, 2)
+        self_eval = target_positions === nothing
+        pos = self_eval ? buf : Matrix{Float64}(target_positions)
+        n_t = self_eval ? n_s : size(pos, 2)
+        sdim = kind === :vortex ? 3 : 1
+        d_str = zeros(Float64, sdim, n_s)
+        d_pos = zeros(Float64, 3, n_s)
+        d_tpos = zeros(Float64, 3, self_eval ? 0 : n_t)
+        fwd = zeros(Float64, 16, n_t)
+        opt = _options(; kwargs...)
+        res = FmmResult()
+        GC.@preserve buf pos fwd Δ d_str d_pos d_tpos begin
+            src = FmmSourceSystem(kind === :vortex ? Cint(3) : Cint(1), n_s, size(buf, 1), pointer(buf), 0)
+            tgt = FmmTargetSystem(n_t, self_eval ? Ptr{Cdouble}(C_NULL) : pointer(pos),
+                                  self_eval ? 0 : size(pos, 1), pointer(fwd), 0)
+            check(ccall((:fmm_vjp, libfmm), Cint,
+                        (Ptr{Cvoid}, Ref{FmmTargetSystem}, Ref{FmmSourceSystem}, Ref{FmmOptions}, Ptr{Cdouble},
+                         Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ref{FmmResult}),
+                        context(), tgt, src, opt, pointer(Δ), pointer(d_str), pointer(d_pos),
+                        self_eval ? Ptr{Cdouble}(C_NULL) : pointer(d_tpos), res))
+        end
+        Δbuf = zeros(Float64, size(buf))
+        Δbuf[1:3, :] .= d_pos
+        Δbuf[5:4+sdim, :] .= d_str
+        Δtargets = self_eval ? ChainRulesCore.NoTangent() : d_tpos
+        return ChainRulesCore.NoTangent(), Δbuf, Δtargets, ChainRulesCore.NoTangent()
+    end
+    return out, fmm_buffer_pullback
 end
 
 end # module

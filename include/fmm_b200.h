@@ -187,9 +187,12 @@ FMM_API int fmm_solve_multi(fmm_ctx* ctx, const fmm_target_system* target, const
  *   vortex particles (kind 3): reads rows 5..7 (u) of d_out, w_t = dL/du_t;
  *     dL/dGamma_s = u_w(x_s), (dL/dx_s)_i = sum_c Gamma_sc du_w,c/dx_i [+ sum_c w_sc
  *     du_c/dx_i when the sources are the targets], (dL/dy_t)_i = sum_c w_tc du_c/dx_i(y_t).
- * Cotangents on the gradient rows of point sources would need dipole sources and are
- * not read.  The result is the exact gradient of the continuous problem evaluated to
- * the FMM's accuracy.  All arrays use source->memory; d_strength holds 1 (kind 1) or 3
+ * Cotangents on rows 1..3 (the target positions echoed into the buffer) pass through
+ * to dL/dy (or dL/dx when the sources are the targets).  A non-zero cotangent on any
+ * other row (the gradient and Hessian rows of point sources, which would need dipole
+ * sources; the potential and velocity-gradient rows of vortex particles) is rejected
+ * with FMM_ERR_ARGUMENT before any work.  The result is the exact gradient of the
+ * continuous problem evaluated to the FMM's accuracy.  All arrays use source->memory; d_strength holds 1 (kind 1) or 3
  * (kind 3) values per source, the position gradients 3 per body; d_target_position
  * may be NULL and is not written when target->positions == NULL. */
 FMM_API int fmm_vjp(fmm_ctx* ctx, const fmm_target_system* target, const fmm_source_system* source,

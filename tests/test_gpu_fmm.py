@@ -88,13 +88,11 @@ def compare_trees(g, o):
 
 
 def compare_lists(gm, gd, om, od):
-    # identical (target, source) pair sets, both sorted by target; order within a target may differ
+    # the reference's lists bit for bit: rows by target (sort_by_target, stable) and, inside a
+    # row, the order of the depth-first recursion
     for a, b in ((gm, om), (gd, od)):
         assert len(a) == len(b)
-        np.testing.assert_array_equal(a[:, 0], b[:, 0])
-        ka = np.lexsort((a[:, 1], a[:, 0]))
-        kb = np.lexsort((b[:, 1], b[:, 0]))
-        np.testing.assert_array_equal(a[ka], b[kb])
+        np.testing.assert_array_equal(a, b)
 
 
 CASES = [
@@ -152,6 +150,8 @@ def test_vortex_ring_velocity_and_gradient(ctx):
     out, res = fm.solve_buffers(buf, L.FMM_POINT_VORTEX, og, ctx=ctx)
     ref = O.fmm(buf, O.POINT_VORTEX, oo, want_tree=True)
     compare_trees(fm.get_tree(ctx, 1), ref["source_tree"])
+    gm, gd = fm.get_lists(ctx)
+    compare_lists(gm, gd, ref["m2l"], ref["direct"])
     for rows in (slice(4, 7), slice(7, 16)):
         scale = np.abs(ref["out"][:, rows]).max()
         np.testing.assert_allclose(out[:, rows], ref["out"][:, rows], rtol=0, atol=1e-10 * scale)
@@ -261,6 +261,8 @@ def test_error_controlled_orders_match_oracle(ctx, em):
         np.testing.assert_allclose(g["max_influence"], ref["target_tree"]["max_influence"], rtol=1e-11, atol=0)
     assert res.p_max == ref["pmax"]
     assert bool(res.error_success) == ref["error_success"]
+    gm, gd = fm.get_lists(ctx)
+    compare_lists(gm, gd, ref["m2l"], ref["direct"])
     scale = np.abs(ref["out"][:, 4:7]).max()
     np.testing.assert_allclose(out[:, 4:7], ref["out"][:, 4:7], rtol=0, atol=1e-10 * scale)
 
@@ -273,6 +275,8 @@ def test_dual_tree_probes(ctx):
     out, res = fm.solve_buffers(src, L.FMM_POINT_SOURCE, og, target_pos=probes, ctx=ctx)
     ref = O.fmm(src, O.POINT_SOURCE, oo, target_pos=probes, want_tree=True)
     compare_trees(fm.get_tree(ctx, 0), ref["target_tree"])
+    gm, gd = fm.get_lists(ctx)
+    compare_lists(gm, gd, ref["m2l"], ref["direct"])
     scale = np.abs(ref["out"][:, 3:7]).max()
     np.testing.assert_allclose(out[:, 3:7], ref["out"][:, 3:7], rtol=0, atol=1e-10 * scale)
 

@@ -52,11 +52,12 @@ def direct_out(ctx, buf, kind, tpos=None):
     return out
 
 
-def loss(ctx, buf, kind, w, tpos=None):
+def loss(ctx, buf, kind, w, tpos=None, wpos=None):
     out = direct_out(ctx, np.ascontiguousarray(buf), kind, None if tpos is None else np.ascontiguousarray(tpos))
+    extra = 0.0 if wpos is None else float(np.sum(wpos * out[:, 0:3]))  # rows 1..3 echo the target positions
     if kind == L.FMM_POINT_SOURCE:
-        return float(np.dot(w, out[:, 3]))
-    return float(np.sum(w * out[:, 4:7]))
+        return float(np.dot(w, out[:, 3])) + extra
+    return float(np.sum(w * out[:, 4:7])) + extra
 
 
 def check(ctx, kind, tpos, seed):
@@ -70,6 +71,9 @@ def check(ctx, kind, tpos, seed):
         d_out[:, 3] = w
     else:
         d_out[:, 4:7] = w
+    # cotangents on the echoed target positions (rows 1..3) pass straight through
+    wpos = 0.1 * rng.standard_normal((nt, 3))
+    d_out[:, 0:3] = wpos
     opt = fm.make_options(expansion_order=14, leaf_size_source=40, multipole_acceptance=0.4, scalar_potential=True)
     out, dstr, dpos, dtp, res = fm.vjp_buffers(buf, kind, opt, d_out, tpos, ctx)
     # the forward buffer is the fmm! result
@@ -85,7 +89,7 @@ def check(ctx, kind, tpos, seed):
             bp, bm = buf.copy(), buf.copy()
             bp[i, 4 + c] += hq
             bm[i, 4 + c] -= hq
-            fd = (loss(ctx, bp, kind, w, tpos) - loss(ctx, bm, kind, w, tpos)) / (2 * hq)
+            fd = (loss(ctx, bp, kind, w, tpos, wpos) - loss(ctx, bm, kind, w, tpos, wpos)) / (2 * hq)
             got = dstr[i] if kind == L.FMM_POINT_SOURCE else dstr[i, c]
             assert abs(got - fd) <= 1e-7 * sc, (i, c, got, fd)
     # source positions
@@ -95,7 +99,7 @@ def check(ctx, kind, tpos, seed):
             bp, bm = buf.copy(), buf.copy()
             bp[i, k] += H
             bm[i, k] -= H
-            fd = (loss(ctx, bp, kind, w, tpos) - loss(ctx, bm, kind, w, tpos)) / (2 * H)
+            fd = (loss(ctx, bp, kind, w, tpos, wpos) - loss(ctx, bm, kind, w, tpos, wpos)) / (2 * H)
             assert abs(dpos[i, k] - fd) <= 2e-6 * sp, (i, k, dpos[i, k], fd)
     # target positions
     if tpos is not None:
@@ -105,7 +109,7 @@ def check(ctx, kind, tpos, seed):
                 tp, tm = tpos.copy(), tpos.copy()
                 tp[i, k] += H
                 tm[i, k] -= H
-                fd = (loss(ctx, buf, kind, w, tp) - loss(ctx, buf, kind, w, tm)) / (2 * H)
+                fd = (loss(ctx, buf, kind, w, tp, wpos) - loss(ctx, buf, kind, w, tm, wpos)) / (2 * H)
                 assert abs(dtp[i, k] - fd) <= 2e-6 * st, (i, k, dtp[i, k], fd)
 
 
@@ -134,3 +138,82 @@ def test_vjp_python_api(ctx):
     buf[:, 4] = w
     psi = direct_out(ctx, buf, L.FMM_POINT_SOURCE)[:, 3]
     np.testing.assert_allclose(r["d_strength"], psi, rtol=0, atol=1e-8 * np.abs(psi).max())
+
+
+@pytest.mark.parametrize("kind", [L.FMM_POINT_SOURCE, L.FMM_POINT_VORTEX], ids=["source", "vortex"])
+def test_vjp_rejects_cotangents_it_cannot_propagate(ctx, kind):
+    # gradient rows of point sources (dipole sources would be needed), the velocity gradient
+    # of vortex particles: an error, not a silently wrong gradient
+    buf = bodies(300, kind, 3)
+    opt = fm.make_options(expansion_order=6, leaf_size_source=30, multipole_acceptance=0.5, scalar_potential=True)
+    d_out = np.zeros((300, 16))
+    d_out[7, 5 if kind == L.FMM_POINT_SOURCE else 9] = 1.0
+    with pytest.raises(L.FMMError) as e:
+        fm.vjp_buffers(buf, kind, opt, d_out, None, ctx)
+    assert e.value.status == L.FMM_ERR_ARGUMENT
+
+
+def test_vjp_mixed_precision_matches_f64(ctx):
+    # the mixed-precision forward and adjoint solves against the FP64 ones
+    n = 20000
+    buf = bodies(n, L.FMM_POINT_SOURCE, 12)
+    rng = np.random.default_rng(13)
+    tpos = np.ascontiguousarray(-0.5 + 2.0 * rng.random((4000, 3)))
+    d_out = np.zeros((4000, 16))
+    d_out[:, 3] = rng.standard_normal(4000)
+    r = {}
+    for prec in ("f64", "mixed"):
+        opt = fm.make_options(expansion_order=8, leaf_size_source=50, multipole_acceptance=0.5,
+                              scalar_potential=True, precision=prec)
+        r[prec] = fm.vjp_buffers(buf, L.FMM_POINT_SOURCE, opt, d_out, tpos, ctx)
+    for k in (1, 2, 3):
+        a, b = r["mixed"][k], r["f64"][k]
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-5, k
+
+
+def test_vjp_adjoint_workload_shape_finite_differences(ctx):
+    # 200k sources U[0,1]^3, 10k probes U[-0.5,1.5]^3, p = 8, L = sum phi^2 (dL/dphi = 2 phi);
+    # central differences of the exact loss (FP64 all-pairs) on 64 coordinates, h = 1e-6
+    rng = np.random.default_rng(4)
+    n, npr = 200_000, 10_000
+    buf = np.zeros((n, 5))
+    buf[:, :3] = rng.random((n, 3))
+    buf[:, 4] = rng.random(n)
+    probes = np.ascontiguousarray(-0.5 + 2.0 * rng.random((npr, 3)))
+    opt = fm.make_options(expansion_order=8, leaf_size_source=50, multipole_acceptance=0.5, scalar_potential=True)
+    out, _ = fm.solve_buffers(buf, L.FMM_POINT_SOURCE, opt, target_pos=probes, ctx=ctx)
+    d_out = np.zeros((npr, 16))
+    d_out[:, 3] = 2.0 * out[:, 3]
+    _, dq, dx, dy, _ = fm.vjp_buffers(buf, L.FMM_POINT_SOURCE, opt, d_out, probes, ctx)
+
+    def lossq(b, pr):
+        o = direct_out(ctx, np.ascontiguousarray(b), L.FMM_POINT_SOURCE, np.ascontiguousarray(pr))
+        return float(np.sum(o[:, 3] ** 2))
+
+    h = 1e-6
+    devs = []
+    for j in range(64):
+        which = j % 3
+        if which == 0:
+            i = rng.integers(0, n)
+            bp, bm = buf.copy(), buf.copy()
+            hq = 1e-3 * buf[i, 4]
+            bp[i, 4] += hq
+            bm[i, 4] -= hq
+            fd = (lossq(bp, probes) - lossq(bm, probes)) / (2 * hq)
+            devs.append(abs(dq[i] - fd) / np.abs(dq).max())
+        elif which == 1:
+            i, k = rng.integers(0, n), rng.integers(0, 3)
+            bp, bm = buf.copy(), buf.copy()
+            bp[i, k] += h
+            bm[i, k] -= h
+            fd = (lossq(bp, probes) - lossq(bm, probes)) / (2 * h)
+            devs.append(abs(dx[i, k] - fd) / np.abs(dx).max())
+        else:
+            i, k = rng.integers(0, npr), rng.integers(0, 3)
+            pp, pm = probes.copy(), probes.copy()
+            pp[i, k] += h
+            pm[i, k] -= h
+            fd = (lossq(buf, pp) - lossq(buf, pm)) / (2 * h)
+            devs.append(abs(dy[i, k] - fd) / np.abs(dy).max())
+    assert max(devs) <= 1e-5, max(devs)
