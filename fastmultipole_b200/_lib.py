@@ -97,6 +97,7 @@ SIGNATURES = {
     "fmm_serve_submit": (C.c_int, [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)]),
     "fmm_serve_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Result), C.c_int]),
     "fmm_serve_stop": (C.c_int, [C.c_void_p]),
+    "fmm_request_footprint": (C.c_size_t, [C.POINTER(Request)]),
     "fmm_direct_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.POINTER(TargetSystem), C.POINTER(SourceSystem), C.c_int,
                                      C.c_int, C.c_int, C.c_int]),
     "fmm_get_tree": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TreeView)]),

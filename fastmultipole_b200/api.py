@@ -442,12 +442,27 @@ def vjp(system, d_potential=None, d_velocity=None, targets=None, *, leaf_size=20
     return r
 
 
+def request_footprint(source_buf, kind, opt, target_pos=None):
+    """Device bytes the serving account reserves for one request (fmm_request_footprint)."""
+    sb = np.ascontiguousarray(source_buf, dtype=np.float64)
+    n_s, d = sb.shape
+    if target_pos is None:
+        tgt = L.TargetSystem(n_s, None, 0, None, L.FMM_MEMORY_HOST)
+    else:
+        tp = np.ascontiguousarray(target_pos, dtype=np.float64)
+        tgt = L.TargetSystem(len(tp), tp.ctypes.data, 3, None, L.FMM_MEMORY_HOST)
+    req = L.Request(tgt, L.SourceSystem(kind, n_s, d, sb.ctypes.data, L.FMM_MEMORY_HOST), opt)
+    return int(L.lib().fmm_request_footprint(C.byref(req)))
+
+
 class Server:
     """Concurrent fmm! requests on one device (fmm_serve_*): ``n_workers`` solver
     contexts run queued requests (oldest first) as soon as one finishes, and
     ``n_workers // 2`` (at least one) express contexts on highest-priority streams run
-    requests of at most 65,536 source plus target bodies; each of these workers has an
-    HBM budget of ``hbm_budget / (n_workers + n_workers // 2)`` (0: unlimited)."""
+    requests of at most 65,536 source plus target bodies.  ``hbm_budget`` (bytes, 0:
+    unlimited) is one account shared by all workers: a request that fits it waits for
+    memory in arrival order; only a request larger than the whole budget fails with
+    FMM_ERR_MEMORY."""
 
     def __init__(self, n_workers=4, hbm_budget=0, ctx=None):
         self.ctx = ctx or default_context()

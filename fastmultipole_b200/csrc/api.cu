@@ -229,6 +229,10 @@ DevBuf<int>& est_stats(fmm_ctx* c) { return c->est_stats; }
 namespace fmmb {
 void*& ctx_serve_slot(fmm_ctx* c) { return c->serve; }
 int ctx_device(fmm_ctx* c) { return c->device; }
+// device memory of a request's solve (an estimate from its sizes and options) and the
+// release of a context's device buffers (serving: memory handed back to the shared account)
+size_t request_footprint(const fmm_request* r);
+void ctx_release_buffers(fmm_ctx* c);
 }  // namespace fmmb
 
 namespace {
@@ -536,6 +540,38 @@ void release_scratch(Scratch& s) {
 }
 
 }  // namespace
+
+namespace fmmb {
+size_t request_footprint(const fmm_request* r) {
+  SolveIn in;
+  in.d = r->source.data_per_body;
+  in.kind = r->source.kind;
+  in.n_s = std::max<int64_t>(0, r->source.n_bodies);
+  in.src = nullptr;
+  in.tpos = r->target.positions;
+  in.t_stride = r->target.stride;
+  in.n_t = r->target.positions ? std::max<int64_t>(0, r->target.n_bodies) : in.n_s;
+  return footprint(in, r->options);
+}
+
+void ctx_release_buffers(fmm_ctx* c) {
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (Workspace* w : {&c->main, &c->est}) {
+    release_tree(w->tree[0]);
+    release_tree(w->tree[1]);
+    release_lists(w->lists);
+    w->acc13.release();
+    w->acc13_far.release();
+  }
+  release_scratch(c->sc);
+  release_scratch(c->est_sc);
+  for (DevBuf<double>* b : {&c->stage_s, &c->stage_t, &c->out16, &c->est_out16, &c->adj_src, &c->adj_out16,
+                            &c->stage_d, &c->vjp_out, &c->multi16})
+    b->release();
+  c->have_solve = false;
+}
+}  // namespace fmmb
 
 extern "C" {
 

@@ -400,11 +400,92 @@ __device__ __forceinline__ void packed_vortex_batch(const float4* __restrict__ B
   }
 }
 
+// The batch holding the target's own leaf on the mixed path runs in FP64: its closest
+// pairs are the ones whose FP32 coordinates relative to the leaf centre (absolute error
+// about 2^-24 of the leaf size) would give large relative errors, and a few such pairs
+// dominate the error of the whole field.  The batch holds per body (x, y, z, q) (point
+// sources) or (x, y, z, G0, G1, G2) (vortex particles) relative to the target leaf
+// centre, in FP64 (the size of the packed FP32 record); the lane's targets are read again
+// in FP64.
+// the lane's two targets relative to the leaf centre in FP64
+__device__ __forceinline__ void self_targets_f64(const double4* __restrict__ tpos, int first, int nt, int ti, int TS,
+                                                 double ox, double oy, double oz, double (&tx)[2], double (&ty)[2],
+                                                 double (&tz)[2]) {
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    tx[k] = ty[k] = tz[k] = 0.0;
+    const int i = ti + k * TS;
+    if (i < nt) {
+      const double4 p = tpos[first + i];
+      tx[k] = p.x - ox;
+      ty[k] = p.y - oy;
+      tz[k] = p.z - oz;
+    }
+  }
+}
+
+template <bool PS, int NA>
+__device__ __noinline__ void self_batch_f64_source(const double4* __restrict__ Bd, int j0, int nb, int SS,
+                                                      const double (&tx)[2], const double (&ty)[2],
+                                                      const double (&tz)[2], double (&tot)[2][NA]) {
+  for (int j = j0; j < nb; j += SS) {
+    const double4 sp = Bd[j];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const double dx = tx[k] - sp.x, dy = ty[k] - sp.y, dz = tz[k] - sp.z;
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 > 0.0) {
+        const double ri = rsqrt(r2);
+        const double qr = sp.w * ri;
+        if (PS) tot[k][0] += qr;
+        const double q3 = qr * ri * ri;
+        tot[k][1 % NA] += dx * q3;
+        tot[k][2 % NA] += dy * q3;
+        tot[k][3 % NA] += dz * q3;
+      }
+    }
+  }
+}
+
+template <bool GS, bool HS, int NA>
+__device__ __noinline__ void self_batch_f64_vortex(const double2* __restrict__ Bd, int j0, int nb, int SS,
+                                                      const double (&tx)[2], const double (&ty)[2],
+                                                      const double (&tz)[2], double (&tot)[2][NA]) {
+  constexpr int h = GS ? 3 : 0;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    double u[3] = {0.0, 0.0, 0.0}, Q[9], E[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int a = 0; a < 9; ++a) Q[a] = 0.0;
+    for (int j = j0; j < nb; j += SS) {
+      const double2 a = Bd[3 * j], b = Bd[3 * j + 1], c = Bd[3 * j + 2];
+      vortex_pair_qe<double, GS>(tx[k], ty[k], tz[k], a.x, a.y, b.x, b.y, c.x, c.y, u, Q, E);
+    }
+    if (GS)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) tot[k][c % NA] += u[c];
+    if (HS) {
+      double gr[9];
+      vortex_grad_from_qe<double>(Q, E, gr);
+#pragma unroll
+      for (int a = 0; a < 9; ++a) tot[k][(h + a) % NA] += gr[a];
+    }
+  }
+}
+
 // RW: one warp per row (rows of small leaves, kWarps rows per CTA), the warp adding its
 // sums to the targets itself; otherwise one CTA per row, the warps splitting its sources.
 // W warps per CTA: kWarps, or kWideWarps for launches of few rows (one long row per CTA).
+// resident CTAs of the mixed instances: the registers the packed loop needs (the FP64
+// branch of the batch holding the target's own leaf is a call, and must not raise them)
+template <class R, int KIND, bool HS, bool RW, int W>
+__host__ __device__ constexpr int p2p_min_blocks() {
+  constexpr int regs = (KIND == FMM_POINT_VORTEX && HS) ? (RW ? 168 : 128) : (RW ? 72 : 64);
+  return sizeof(R) != 4 ? 1 : (65536 / (regs * W * 32) > 0 ? 65536 / (regs * W * 32) : 1);
+}
+
 template <class R, int KIND, bool PS, bool GS, bool HS, bool RW, int W = kWarps>
-__global__ void __launch_bounds__(W * 32) k_p2p(const int* __restrict__ tgt_list, const int* __restrict__ off,
+__global__ void __launch_bounds__(W * 32, p2p_min_blocks<R, KIND, HS, RW, W>()) k_p2p(const int* __restrict__ tgt_list, const int* __restrict__ off,
                                                      int n_rows, const int* __restrict__ src_of,
                                                      const int* __restrict__ t_start, const int* __restrict__ t_count,
                                                      const double* __restrict__ t_center,
@@ -515,7 +596,20 @@ __global__ void __launch_bounds__(W * 32) k_p2p(const int* __restrict__ tgt_list
         }
         const int ek = __shfl_sync(kAll, excl, k);
         const int sk = __shfl_sync(kAll, sb, k);
-        if (PACK && idx < nb) {
+        if ((PACK || PACKV) && self_batch && idx < nb) {
+          // FP64 (x, y, z, q) / (x, y, z, G0), (G1, G2, -, -) relative to the target leaf centre
+          const int body = sk + idx - ek;
+          const double4 p = spos[body];
+          const double4 g = sstr[body];
+          if (PACK) {
+            reinterpret_cast<double4*>(B)[idx] = make_double4(p.x - ox, p.y - oy, p.z - oz, g.x);
+          } else {  // 48 bytes per body, the size of the packed FP32 record
+            double2* Bd = reinterpret_cast<double2*>(B) + 3 * idx;
+            Bd[0] = make_double2(p.x - ox, p.y - oy);
+            Bd[1] = make_double2(p.z - oz, g.x);
+            Bd[2] = make_double2(g.y, g.z);
+          }
+        } else if (PACK && idx < nb) {
           const int body = sk + idx - ek;
           const double4 p = spos[body];
           const float x = -(float)(p.x - ox), y = -(float)(p.y - oy), z = -(float)(p.z - oz), q = (float)sstr[body].x;
@@ -554,11 +648,13 @@ __global__ void __launch_bounds__(W * 32) k_p2p(const int* __restrict__ tgt_list
         const float2 ty2 = make_float2((float)ty[0], (float)ty[1]);
         const float2 tz2 = make_float2((float)tz[0], (float)tz[1]);
         float2 ph = make_float2(0.f, 0.f), gx = ph, gy = ph, gz = ph;
-        // pairs with r^2 = 0 (coincident bodies) are skipped: batches holding the target's own
-        // leaf guard every pair; the others run unguarded and, in the rare case that their sums
-        // come out non-finite, repeat the batch with the guard (the same result either way)
+        // the batch holding the target's own leaf runs in FP64 and skips coincident bodies;
+        // the others run unguarded and, in the rare case that their sums come out non-finite
+        // (bodies that coincide in FP32), repeat the batch with the r^2 > 0 guard
         if (self_batch) {
-          packed_batch<true, PS>(B4, slice, nb, SS, tx2, ty2, tz2, ph, gx, gy, gz);
+          double txd[2], tyd[2], tzd[2];
+          self_targets_f64(tpos, ts + tile, nt, ti, TS, ox, oy, oz, txd, tyd, tzd);
+          self_batch_f64_source<PS, NA>(reinterpret_cast<const double4*>(B), slice, nb, SS, txd, tyd, tzd, tot);
         } else {
           packed_batch<false, PS>(B4, slice, nb, SS, tx2, ty2, tz2, ph, gx, gy, gz);
           if (!isfinite(ph.x + ph.y + gx.x + gx.y + gy.x + gy.y + gz.x + gz.y)) {
@@ -580,9 +676,13 @@ __global__ void __launch_bounds__(W * 32) k_p2p(const int* __restrict__ tgt_list
         const float2 tz2 = make_float2((float)tz[0], (float)tz[1]);
         const float4* B4 = reinterpret_cast<const float4*>(B);
         float2 acc[NA];
-        // as on the point-source path: only batches holding the target's own leaf guard every pair
+        // as on the point-source path: the batch holding the target's own leaf runs in FP64
         if (self_batch) {
-          packed_vortex_batch<true, GS, HS, NA>(B4, slice, nb, SS, tx2, ty2, tz2, acc);
+#pragma unroll
+          for (int a = 0; a < NA; ++a) acc[a] = make_float2(0.f, 0.f);
+          double txd[2], tyd[2], tzd[2];
+          self_targets_f64(tpos, ts + tile, nt, ti, TS, ox, oy, oz, txd, tyd, tzd);
+          self_batch_f64_vortex<GS, HS, NA>(reinterpret_cast<const double2*>(B), slice, nb, SS, txd, tyd, tzd, tot);
         } else {
           packed_vortex_batch<false, GS, HS, NA>(B4, slice, nb, SS, tx2, ty2, tz2, acc);
           float sum = 0.f;

@@ -206,9 +206,11 @@ FMM_API int fmm_vjp(fmm_ctx* ctx, const fmm_target_system* target, const fmm_sou
  * worker takes the oldest queued request as soon as it finishes one.  n_workers / 2
  * (at least one) express workers besides take only requests of at most 65,536 source
  * plus target bodies, on highest-priority streams, so that small requests do not wait
- * behind large ones.  Each of the n_workers + n_workers / 2 workers has an HBM
- * budget of hbm_budget_bytes / their number (0 = unlimited); a request that does not fit
- * finishes with FMM_ERR_MEMORY.  A request's result does not depend on what else is
+ * behind large ones.  Device memory is one account of hbm_budget_bytes shared by all
+ * workers (0 = unlimited): a request whose estimated footprint fits the budget waits,
+ * in arrival order, until the memory held by the other workers' buffers (which they
+ * hand back while someone waits) leaves room for it; only a request larger than the
+ * whole budget finishes with FMM_ERR_MEMORY.  A request's result does not depend on what else is
  * running (each request runs the deterministic fmm_solve path on its own buffers).
  * The caller keeps every buffer of a request alive until fmm_serve_poll has
  * returned something other than FMM_PENDING for its id; each id is polled to
@@ -226,6 +228,8 @@ FMM_API int fmm_serve_submit(fmm_ctx* ctx, const fmm_request* request, uint64_t*
 FMM_API int fmm_serve_poll(fmm_ctx* ctx, uint64_t id, fmm_result* result, int timeout_ms);
 /* finishes the queued requests, then stops the workers */
 FMM_API int fmm_serve_stop(fmm_ctx* ctx);
+/* the device-memory estimate the serving account reserves for a request (bytes) */
+FMM_API size_t fmm_request_footprint(const fmm_request* request);
 
 /* ---- direct! without device allocations --------------------------------------
  * No counterpart in the reference: an all-pairs direct! (same kernels as

@@ -86,8 +86,8 @@ def test_pending_errors_and_budget():
         if rc == L.FMM_PENDING:
             rc, out, _ = server.poll(rid, timeout_ms=-1)
         assert rc == L.FMM_OK and np.isfinite(out[:, 4:7]).all()
-        # a request above one worker's share of the budget (2 GB over 2 + 1 workers) fails alone
-        huge = bodies(4_000_000, 1, 12)
+        # a request larger than the whole budget fails alone
+        huge = bodies(8_000_000, 1, 12)
         rid = server.submit(huge, 1, opt)
         assert server.poll(rid)[0] == L.FMM_ERR_MEMORY
         # an invalid request fails with its own status; the next one still runs
@@ -99,5 +99,25 @@ def test_pending_errors_and_budget():
         server.stop()
         with pytest.raises(fm.FMMError):
             server.submit(bodies(10, 1, 15), 1, opt)
+    finally:
+        ctx.close()
+
+
+def test_requests_wait_for_memory_instead_of_failing():
+    # a budget that holds one of these requests but not three: each one fits (it waits for
+    # the memory the others hand back), none fails, and the results equal the solves alone
+    ctx = fm.Context(0)
+    try:
+        opt = fm.make_options(expansion_order=8, leaf_size_source=64, multipole_acceptance=0.5)
+        bufs = [bodies(900_000, 1, 20 + k) for k in range(3)]
+        alone = [fm.solve_buffers(b, 1, opt, ctx=ctx)[0] for b in bufs]
+        budget = int(1.5 * fm.request_footprint(bufs[0], 1, opt))
+        server = fm.Server(n_workers=3, hbm_budget=budget, ctx=ctx)
+        ids = [server.submit(b, 1, opt) for b in bufs]
+        for k, rid in enumerate(ids):
+            rc, out, _ = server.poll(rid, timeout_ms=-1)
+            assert rc == L.FMM_OK
+            np.testing.assert_array_equal(out, alone[k])
+        server.stop()
     finally:
         ctx.close()
