@@ -363,8 +363,8 @@ def solve_buffers(source_buf, kind, opt, target_pos=None, ctx=None, timing=False
 
 
 def solve_multi_buffers(sources, opt, target_pos, ctx=None):
-    """fmm! of several source systems on raw buffers: ``sources`` is a list of
-    (buffer (N_k, d_k), kind); the target buffers of the per-system solves are summed
+    """fmm! of a tuple of source systems on raw buffers: ``sources`` is a list of
+    (buffer (N_k, d_k), kind) in tuple order; one octree over all of their bodies
     (fmm_solve_multi).  Returns (out (Nt, 16), fmm_result)."""
     ctx = ctx or default_context()
     bufs = [np.ascontiguousarray(b, dtype=np.float64) for b, _ in sources]
@@ -523,17 +523,17 @@ def fmm(target_systems, source_systems=None, *, leaf_size=None, leaf_size_source
                        nearfield, self_induced, upward_pass, horizontal_pass, downward_pass, scalar_potential,
                        gradient, hessian, precision)
     if len({s.kernel for s in sources}) > 1:
-        # systems of different kernels: one solve per kernel on the same targets, summed
-        groups = {}
-        for s in sources:
-            groups.setdefault(_kind((s,)), []).append(s)
-        out, res = solve_multi_buffers([(_source_buffer(g, k), k) for k, g in groups.items()], opt,
+        # systems of different kernels: one octree over all of them (Tree(systems::Tuple),
+        # src/tree.jl:3-122), the systems in tuple order
+        out, res = solve_multi_buffers([(_source_buffer((s,), _kind((s,))), _kind((s,))) for s in sources], opt,
                                        _positions(targets), ctx)
         switch = DerivativesSwitch(bool(scalar_potential), bool(gradient), bool(hessian))
         _scatter(targets, out, switch)
+        m2l, dl = get_lists(ctx)
         optimized = dict(leaf_size_source=ls_s, expansion_order=max(expansion_order, 1),
                          multipole_acceptance=multipole_acceptance)
-        return (optimized, ctx, None, None, None, None, tuple(switch for _ in targets), bool(res.error_success))
+        return (optimized, ctx, TreeHandle(ctx, 0), TreeHandle(ctx, 1), m2l, dl, tuple(switch for _ in targets),
+                bool(res.error_success))
     kind = _kind(sources)
     buf = _source_buffer(sources, kind)
     same = self_eval or all(a is b for a, b in zip(targets, sources)) and len(targets) == len(sources)

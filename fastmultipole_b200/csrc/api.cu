@@ -13,15 +13,29 @@
 #include <cstring>
 #include <string>
 
+#include <cub/cub.cuh>
+
 #include "context.cuh"
 
 using namespace fmmb;
 
 namespace {
 
+// One source system's bodies inside a tuple's shared octree (Tree(systems::Tuple, ...),
+// src/tree.jl:3-122 keeps one buffer per system and per branch one body range per system):
+// the system's bodies in tree order, and per branch the range of them it holds.
+struct SysView {
+  int kind = FMM_POINT_SOURCE;
+  int64_t n = 0;
+  DevBuf<double4> pos, str;
+  DevBuf<int> start, count, pre;
+};
+
 struct Workspace {
   DevTree tree[2];  // [0] target role, [1] source role (aliased when shared)
   DevLists lists;
+  DevBuf<int> sys_orig, sys_sorted;  // tuples: system of every source body (input / tree order)
+  SysView views[8];
   DevBuf<double> acc13;      // target buffer rows 4..16, sorted order: near field (the whole field
                              // when the far field runs on the same stream)
   DevBuf<double> acc13_far;  // far field (L2P) when it runs on the far-field stream
@@ -74,6 +88,49 @@ __device__ __host__ inline bool vjp_unsupported_row(int kind, int r) {
 __global__ void k_check_cotangents(int64_t n, int kind, const double* __restrict__ dout16, int* __restrict__ flag) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 16 * n; i += (int64_t)gridDim.x * blockDim.x)
     if (vjp_unsupported_row(kind, (int)(i % 16)) && dout16[i] != 0.0) atomicExch(flag, 1);
+}
+
+// tuple of systems: system k's bodies into the shared body arrays at offset off (rows of
+// the reference buffer: x, y, z, radius, strength), with the system index of each
+__global__ void k_unpack_system(const double* __restrict__ buf, int64_t n, int d, int kind, int64_t off, int k,
+                                double4* __restrict__ pos, double4* __restrict__ str, int* __restrict__ sys) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double* b = buf + i * d;
+    pos[off + i] = make_double4(b[0], b[1], b[2], b[3]);
+    str[off + i] = kind == FMM_POINT_VORTEX ? make_double4(b[4], b[5], b[6], 0.0) : make_double4(b[4], 0.0, 0.0, 0.0);
+    sys[off + i] = k;
+  }
+}
+
+__global__ void k_gather_int(const int* __restrict__ in, const int* __restrict__ idx, int64_t n, int* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = in[idx[i]];
+}
+
+__global__ void k_flag_system(const int* __restrict__ sys, int64_t n, int k, int* __restrict__ flag) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x)
+    flag[i] = i < n && sys[i] == k;
+}
+
+// system k's bodies in tree order (pre = exclusive count of its bodies before each position)
+__global__ void k_split_system(const int* __restrict__ sys, const int* __restrict__ pre, int64_t n, int k,
+                               const double4* __restrict__ pos, const double4* __restrict__ str,
+                               double4* __restrict__ pos_k, double4* __restrict__ str_k) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (sys[i] == k) {
+      pos_k[pre[i]] = pos[i];
+      str_k[pre[i]] = str[i];
+    }
+}
+
+// per branch, the range of system k's bodies (contiguous in its tree-ordered array)
+__global__ void k_branch_ranges(const int* __restrict__ body_start, const int* __restrict__ body_count, int nb,
+                                const int* __restrict__ pre, int* __restrict__ start, int* __restrict__ count) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+    const int a = pre[body_start[i]], e = pre[body_start[i] + body_count[i]];
+    start[i] = a;
+    count[i] = e - a;
+  }
 }
 
 int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); }
@@ -242,6 +299,15 @@ int fail(fmm_ctx* c, const Error& e) {
   return e.code;
 }
 
+constexpr int kMaxSystems = 8;  // source systems of one tuple
+
+struct SysIn {
+  const double* buf;  // device, body-major d*n
+  int d;
+  int kind;
+  int64_t n;
+};
+
 struct SolveIn {
   const double* src;  // device, body-major d*n_s
   int d;
@@ -250,6 +316,10 @@ struct SolveIn {
   const double* tpos;  // device, stride (nullptr: the sources are the targets)
   int64_t t_stride;
   int64_t n_t;
+  // a tuple of source systems (n_sys > 1): one octree over all their bodies (n_s in total);
+  // src, d and kind are then unused
+  int n_sys = 1;
+  SysIn sys[kMaxSystems] = {};
 };
 
 size_t footprint(const SolveIn& in, const fmm_options& o) {
@@ -279,10 +349,84 @@ DevBuf<int>& est_stats(fmm_ctx* c);
 // the relative error methods, src/fmm.jl:1189-1276, which runs on its own stream) while
 // the near field runs on st; st waits for the far field before the unsort.  The
 // estimate's own sub-solve keeps every stage on its stream.
+// ---- tuples of source systems: one octree over every system's bodies
+// the bodies of all systems, concatenated in tuple order, with the system of each
+void unpack_tuple(Workspace& W, DevTree& S, const SolveIn& in, cudaStream_t st) {
+  S.n_bodies = in.n_s;
+  S.pos.grow(in.n_s);
+  S.str.grow(in.n_s);
+  W.sys_orig.grow(in.n_s);
+  int64_t off = 0;
+  for (int k = 0; k < in.n_sys; ++k) {
+    const SysIn& y = in.sys[k];
+    if (y.n > 0) {
+      note_launch();
+      k_unpack_system<<<grid_for(y.n), 256, 0, st>>>(y.buf, y.n, y.d, y.kind, off, k, S.pos.ptr, S.str.ptr,
+                                                     W.sys_orig.ptr);
+      FMM_CUDA_TRY(cudaGetLastError());
+    }
+    off += y.n;
+  }
+}
+
+// after the tree: every system's bodies in tree order and its body range per branch (the
+// reference's per-system bodies_index; within a leaf the tree keeps input order, so the
+// systems come one after another)
+void build_views(Workspace& W, const DevTree& S, const SolveIn& in, Scratch& sc, cudaStream_t st) {
+  const int64_t n = S.n_bodies;
+  W.sys_sorted.grow(n);
+  note_launch();
+  k_gather_int<<<grid_for(n), 256, 0, st>>>(W.sys_orig.ptr, S.sort_index.ptr, n, W.sys_sorted.ptr);
+  FMM_CUDA_TRY(cudaGetLastError());
+  sc.tmp_i.grow((size_t)n + 1);
+  for (int k = 0; k < in.n_sys; ++k) {
+    SysView& v = W.views[k];
+    v.kind = in.sys[k].kind;
+    v.n = in.sys[k].n;
+    v.pre.grow((size_t)n + 1);
+    v.pos.grow(std::max<int64_t>(v.n, 1));
+    v.str.grow(std::max<int64_t>(v.n, 1));
+    v.start.grow((size_t)S.n_branches);
+    v.count.grow((size_t)S.n_branches);
+    note_launch();
+    k_flag_system<<<grid_for(n + 1), 256, 0, st>>>(W.sys_sorted.ptr, n, k, sc.tmp_i.ptr);
+    size_t tb = 0;
+    FMM_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, sc.tmp_i.ptr, v.pre.ptr, (int)(n + 1), st));
+    sc.cub.grow(tb);
+    note_launch();
+    FMM_CUDA_TRY(cub::DeviceScan::ExclusiveSum(sc.cub.ptr, tb, sc.tmp_i.ptr, v.pre.ptr, (int)(n + 1), st));
+    note_launch();
+    k_split_system<<<grid_for(n), 256, 0, st>>>(W.sys_sorted.ptr, v.pre.ptr, n, k, S.pos.ptr, S.str.ptr, v.pos.ptr,
+                                                v.str.ptr);
+    note_launch();
+    k_branch_ranges<<<grid_for(S.n_branches), 256, 0, st>>>(S.body_start.ptr, S.body_count.ptr, (int)S.n_branches,
+                                                            v.pre.ptr, v.start.ptr, v.count.ptr);
+    FMM_CUDA_TRY(cudaGetLastError());
+  }
+}
+
+// the shared source tree seen through one system's bodies (a non-owning copy: its buffers
+// are never grown or released)
+DevTree view_tree(const DevTree& S, const SysView& v) {
+  DevTree t = S;
+  t.n_bodies = v.n;
+  t.body_start.ptr = v.start.ptr;
+  t.body_count.ptr = v.count.ptr;
+  t.pos.ptr = v.pos.ptr;
+  t.str.ptr = v.str.ptr;
+  return t;
+}
+
 void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, double* out16, fmm_result* res,
              bool is_estimate, cudaStream_t st, Scratch& sc, DevBuf<int>& stats) {
   const int p = o.expansion_order;
-  const bool lh = in.kind == FMM_POINT_VORTEX;
+  const bool multi = in.n_sys > 1;
+  // lamb_helmholtz = has_vector_potential(source_systems) (src/fmm.jl:927)
+  bool lh = in.kind == FMM_POINT_VORTEX;
+  if (multi) {
+    lh = false;
+    for (int k = 0; k < in.n_sys; ++k) lh = lh || in.sys[k].kind == FMM_POINT_VORTEX;
+  }
   const int64_t ls_s = o.leaf_size_source;
   const int64_t ls_t = o.leaf_size_target > 0 ? o.leaf_size_target : ls_s;
   const bool ps = o.scalar_potential != 0, gs = o.gradient != 0, hs = o.hessian != 0;
@@ -299,8 +443,20 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   mark(0);
   // ---- trees (src/tree.jl:3-122)
   DevTree& S = W.tree[1];
-  unpack_bodies(S, in.src, in.n_s, in.d, in.kind, true, st);
+  if (multi)
+    unpack_tuple(W, S, in, st);
+  else
+    unpack_bodies(S, in.src, in.n_s, in.d, in.kind, true, st);
   build_tree(S, sc, st, ls_s, o.list_method, o.shrink_recenter != 0);
+  if (multi) build_views(W, S, in, sc, st);
+  // body_to_multipole! and direct! run per source system (src/fmm.jl:291-346, 3-40)
+  auto p2m_all = [&](cudaStream_t s_) {
+    if (!multi) return launch_p2m(S, p, in.kind, c->tables, s_);
+    for (int k = 0; k < in.n_sys; ++k) {
+      DevTree v = view_tree(S, W.views[k]);
+      launch_p2m(v, p, W.views[k].kind, c->tables, s_);
+    }
+  };
   W.shared = (in.tpos == nullptr) && (ls_t == ls_s);
   if (!W.shared) {
     DevTree& T = W.tree[0];
@@ -334,7 +490,7 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   }
   markf(0);
   if (o.upward_pass && split) {
-    launch_p2m(S, p, in.kind, c->tables, fs);
+    p2m_all(fs);
     launch_m2m(S, p, lh, c->tables, fs);
   }
   markf(1);
@@ -364,10 +520,18 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   if (estimate || split) FMM_CUDA_TRY(cudaEventRecord(fork_event(c), st));
   if (split) FMM_CUDA_TRY(cudaStreamWaitEvent(fs, fork_event(c), 0));
   // near field
-  launch_p2p(T, S, W.lists, W.acc13.ptr, in.kind, ps, gs, hs, o.precision, st);
+  if (!multi) {
+    launch_p2p(T, S, W.lists, W.acc13.ptr, in.kind, ps, gs, hs, o.precision, st);
+  } else {
+    for (int k = 0; k < in.n_sys; ++k) {
+      if (W.views[k].n == 0) continue;
+      DevTree v = view_tree(S, W.views[k]);
+      launch_p2p(T, v, W.lists, W.acc13.ptr, W.views[k].kind, ps, gs, hs, o.precision, st);
+    }
+  }
   mark(3);
   if (o.upward_pass && !split) {
-    launch_p2m(S, p, in.kind, c->tables, st);
+    p2m_all(st);
     launch_m2m(S, p, lh, c->tables, st);
   }
   if (!split) mark(4);
@@ -761,71 +925,78 @@ int fmm_solve_multi(fmm_ctx* c, const fmm_target_system* target, const fmm_sourc
   if (n_sources == 1 && sources) return fmm_solve(c, target, sources, opt, result);
   try {
     FMM_CHECK(sources && n_sources > 1, FMM_ERR_ARGUMENT, "fmm_solve_multi: no source systems");
+    FMM_CHECK(n_sources <= kMaxSystems, FMM_ERR_ARGUMENT, "fmm_solve_multi: at most 8 source systems");
     FMM_CHECK(target && target->positions, FMM_ERR_ARGUMENT,
               "fmm_solve_multi: several source systems need explicit target positions");
     FMM_CHECK(target->stride >= 3, FMM_ERR_ARGUMENT, "target stride must be >= 3");
     FMM_CHECK(opt != nullptr, FMM_ERR_ARGUMENT, "options are NULL");
+    check_options(*opt);
+    FMM_CHECK(opt->list_method != FMM_LIST_BARBA, FMM_ERR_ARGUMENT,
+              "fmm_solve_multi: the Barba rule splits on per-system counts, which is not supported");
     const int64_t nt = target->n_bodies;
     FMM_CHECK(nt >= 0, FMM_ERR_ARGUMENT, "negative target n_bodies");
     FMM_CHECK(nt == 0 || target->out, FMM_ERR_ARGUMENT, "target out buffer is NULL");
-    FMM_CUDA_TRY(cudaSetDevice(c->device));
-    fmm_result total;
-    std::memset(&total, 0, sizeof(total));
-    total.error_success = 1;
-    // every solve sees device-resident targets: the positions (staged once) and an output buffer
-    fmm_target_system td = *target;
-    td.memory = FMM_MEMORY_DEVICE;
-    if (nt > 0) {
-      c->multi16.grow(16 * (size_t)nt);
-      c->vjp_out.grow(16 * (size_t)nt);
-      if (target->memory == FMM_MEMORY_HOST) {
-        c->stage_d.grow(3 * (size_t)nt);
-        FMM_CUDA_TRY(cudaMemcpy2DAsync(c->stage_d.ptr, 3 * sizeof(double), target->positions,
-                                       target->stride * sizeof(double), 3 * sizeof(double), nt,
-                                       cudaMemcpyHostToDevice, c->stream));
-        td.positions = c->stage_d.ptr;
-        td.stride = 3;
-      }
-    }
+    SolveIn in;
+    in.n_sys = n_sources;
+    in.n_s = 0;
     for (int k = 0; k < n_sources; ++k) {
-      td.out = k == 0 ? c->multi16.ptr : c->vjp_out.ptr;
-      fmm_result r;
-      std::memset(&r, 0, sizeof(r));
-      const int rc = fmm_solve(c, &td, &sources[k], opt, &r);
-      if (rc != FMM_OK) return rc;
-      if (nt > 0 && k > 0) {
-        note_launch();
-        k_add_rows<<<grid_for(13 * nt), 256, 0, c->stream>>>(nt, c->vjp_out.ptr, c->multi16.ptr);
-        FMM_CUDA_TRY(cudaGetLastError());
+      check_source(&sources[k]);
+      in.n_s += sources[k].n_bodies;
+    }
+    FMM_CUDA_TRY(cudaSetDevice(c->device));
+    if (result) std::memset(result, 0, sizeof(*result));
+    in.kind = sources[0].kind;
+    in.d = sources[0].data_per_body;
+    in.src = nullptr;
+    in.n_t = nt;
+    in.t_stride = target->stride;
+    in.tpos = nullptr;
+    if (c->budget) FMM_CHECK(footprint(in, *opt) <= c->budget, FMM_ERR_MEMORY, "request exceeds the context's HBM budget");
+    c->have_solve = false;
+    if (in.n_s == 0 || nt == 0) {
+      if (nt > 0) {
+        if (target->memory == FMM_MEMORY_DEVICE) {
+          FMM_CUDA_TRY(cudaMemset2DAsync(target->out + 3, 16 * sizeof(double), 0, 13 * sizeof(double), nt,
+                                         c->stream));
+          FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        } else {
+          for (int64_t i = 0; i < nt; ++i) std::memset(target->out + 16 * i + 3, 0, 13 * sizeof(double));
+        }
       }
-      total.p_max = std::max(total.p_max, r.p_max);
-      total.error_success = total.error_success && r.error_success;
-      total.n_target_branches += r.n_target_branches;
-      total.n_source_branches += r.n_source_branches;
-      total.n_target_leaves += r.n_target_leaves;
-      total.n_source_leaves += r.n_source_leaves;
-      total.n_m2l += r.n_m2l;
-      total.n_direct += r.n_direct;
-      total.n_p2p_pairs += r.n_p2p_pairs;
-      total.m2l_flops += r.m2l_flops;
-      total.t_total_ms += r.t_total_ms;
-      total.t_tree_ms += r.t_tree_ms;
-      total.t_lists_ms += r.t_lists_ms;
-      total.t_influence_ms += r.t_influence_ms;
-      total.t_nearfield_ms += r.t_nearfield_ms;
-      total.t_upward_ms += r.t_upward_ms;
-      total.t_horizontal_ms += r.t_horizontal_ms;
-      total.t_downward_ms += r.t_downward_ms;
-      total.n_kernel_launches += r.n_kernel_launches;
+      if (result) result->error_success = 1;
+      return FMM_OK;
     }
-    if (nt > 0) {
-      const cudaMemcpyKind dir =
-          target->memory == FMM_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-      FMM_CUDA_TRY(cudaMemcpyAsync(target->out, c->multi16.ptr, 16 * (size_t)nt * sizeof(double), dir, c->stream));
-      FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    // every system's buffer on the device (one staging area, systems back to back)
+    size_t total = 0;
+    for (int k = 0; k < n_sources; ++k) total += (size_t)sources[k].data_per_body * sources[k].n_bodies;
+    const bool any_host = [&] {
+      for (int k = 0; k < n_sources; ++k)
+        if (sources[k].memory != FMM_MEMORY_DEVICE) return true;
+      return false;
+    }();
+    if (any_host) c->stage_s.grow(total + 1);
+    size_t at = 0;
+    for (int k = 0; k < n_sources; ++k) {
+      const fmm_source_system& y = sources[k];
+      const size_t nd = (size_t)y.data_per_body * y.n_bodies;
+      const double* dev = y.buffer;
+      if (y.memory != FMM_MEMORY_DEVICE && nd > 0) {
+        FMM_CUDA_TRY(cudaMemcpyAsync(c->stage_s.ptr + at, y.buffer, nd * sizeof(double), cudaMemcpyHostToDevice,
+                                     c->stream));
+        dev = c->stage_s.ptr + at;
+      }
+      in.sys[k] = SysIn{dev, y.data_per_body, y.kind, y.n_bodies};
+      at += nd;
     }
-    c->have_solve = false;  // the exported trees would be those of the last system only
-    if (result) *result = total;
+    in.tpos = stage(c, c->stage_t, target->positions, (size_t)target->stride * nt, target->memory);
+    c->out16.grow(16 * (size_t)nt);
+    run_fmm(c, c->main, in, *opt, c->out16.ptr, result, false, c->stream, c->sc, c->stats);
+    const cudaMemcpyKind dir = target->memory == FMM_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    FMM_CUDA_TRY(cudaMemcpyAsync(target->out, c->out16.ptr, 16 * (size_t)nt * sizeof(double), dir, c->stream));
+    FMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->have_solve = true;
+    c->last_p = opt->expansion_order;
+    c->last_kind = in.kind;
     return FMM_OK;
   } catch (const Error& e) {
     return fail(c, e);

@@ -161,13 +161,16 @@ FMM_API int fmm_direct(fmm_ctx* ctx, const fmm_target_system* target, const fmm_
 
 /* ---- several source systems -----------------------------------------------------
  * fmm!(targets, (system_1, system_2, ...)) with systems of different kernels (point
- * sources and vortex particles, src/fmm.jl:807-884 with tuples of systems).  The field
- * is linear in the sources, so the solve runs once per source system on the same
- * targets and the target buffers are summed (rows 4..16).  The reference instead
- * builds one octree over the bodies of all systems; the two agree to the FMM's
- * accuracy, not to the last digit.  target->positions must be given when
- * n_sources > 1; n_sources == 1 is fmm_solve.  The result reports the largest order
- * used, success only if every solve met its tolerance, and summed counts and times. */
+ * sources and vortex particles, src/fmm.jl:807-884 with tuples of systems): one octree
+ * over the bodies of all systems, as Tree(systems::Tuple, ...) (src/tree.jl:3-122)
+ * builds it, with per branch one body range per system; body_to_multipole! and direct!
+ * run per system, the translations once, with the Lamb-Helmholtz form when any system
+ * is a vortex system (src/fmm.jl:927; the reference warns that the scalar potential is
+ * then not meaningful).  Splits follow the total body count (the TreeStop and
+ * SelfTuning rules with one leaf size); the Barba rule, which splits on per-system
+ * counts, is rejected (FMM_ERR_ARGUMENT).  At most 8 systems; target->positions must
+ * be given when n_sources > 1; n_sources == 1 is fmm_solve.  fmm_get_tree / _lists
+ * export the shared trees and lists of the last call. */
 FMM_API int fmm_solve_multi(fmm_ctx* ctx, const fmm_target_system* target, const fmm_source_system* sources,
                             int n_sources, const fmm_options* options, fmm_result* result);
 

@@ -589,8 +589,14 @@ static oracle_run* fmm_impl(const double* target_pos, int64_t n_t, const double*
                             int kind, int64_t n_s, const oracle_options& o,
                             const std::vector<double>*) {
   if (!source_buf && n_s > 0) return nullptr;
-  if (kind != ORACLE_POINT_SOURCE && kind != ORACLE_POINT_VORTEX) return nullptr;
-  if (d < 4 + kind) return nullptr;
+  // a tuple of systems (Tree(systems::Tuple, ...), src/tree.jl:3-122): one octree over the
+  // bodies of every system, concatenated in tuple order, each body with its kind in row 8.
+  // The octree splits on the total count, as the reference's TreeStop/SelfTuning rules do for
+  // systems of one leaf size; Barba splits on per-system counts and is not restated here.
+  const bool per_body = kind == ORACLE_KIND_PER_BODY;
+  if (kind != ORACLE_POINT_SOURCE && kind != ORACLE_POINT_VORTEX && !per_body) return nullptr;
+  if (d < (per_body ? 8 : 4 + kind)) return nullptr;
+  if (per_body && o.list_method == ORACLE_LIST_BARBA) return nullptr;
   if (o.expansion_order < 1 || o.expansion_order > 40) return nullptr;
   auto run = std::make_unique<oracle_run>();
   run->same = (target_pos == nullptr);
@@ -599,7 +605,10 @@ static oracle_run* fmm_impl(const double* target_pos, int64_t n_t, const double*
   if (run->same) n_t = n_s;
   int p = o.expansion_order;
   int64_t ls_s = o.leaf_size_source, ls_t = o.leaf_size_target > 0 ? o.leaf_size_target : ls_s;
+  // lamb_helmholtz = has_vector_potential(source_systems) (src/fmm.jl:927): any vortex system
   bool lh = (kind == ORACLE_POINT_VORTEX);
+  if (per_body)
+    for (int64_t j = 0; j < n_s && !lh; ++j) lh = source_buf[(int64_t)d * j + 7] == ORACLE_POINT_VORTEX;
   bool ps = o.scalar_potential, gs = o.gradient, hs = o.hessian;
   g_threads = o.n_threads;
   tables(p);  // grow the constant tables before the threaded passes
@@ -650,7 +659,7 @@ static oracle_run* fmm_impl(const double* target_pos, int64_t n_t, const double*
           for (int64_t j = sb.body_start; j < sb.body_start + sb.body_count; ++j) {
             const double* s = &ST.buf[(int64_t)d * j];
             for (int64_t i = tb.body_start; i < tb.body_start + tb.body_count; ++i)
-              p2p(kind, &TT.buf[16 * i], &TT.buf[16 * i + 3], s, gs, hs);
+              p2p(per_body ? (int)s[7] : kind, &TT.buf[16 * i], &TT.buf[16 * i + 3], s, gs, hs);
           }
         }
       });
@@ -667,7 +676,8 @@ static oracle_run* fmm_impl(const double* target_pos, int64_t n_t, const double*
         for (int64_t j = b.body_start; j < b.body_start + b.body_count; ++j) {
           const double* s = &ST.buf[(int64_t)d * j];
           double dx = s[0] - b.source_center[0], dy = s[1] - b.source_center[1], dz = s[2] - b.source_center[2];
-          if (lh)
+          // body_to_multipole! of the body's own system (src/bodytomultipole.jl:387-489)
+          if ((per_body ? (int)s[7] : kind) == ORACLE_POINT_VORTEX)
             p2m_point_vortex(M, w.harm.data(), dx, dy, dz, s[4], s[5], s[6], p);
           else
             p2m_point_source(M, w.harm.data(), dx, dy, dz, s[4], p);

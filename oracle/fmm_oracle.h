@@ -26,6 +26,9 @@ extern "C" {
 #endif
 
 enum { ORACLE_POINT_SOURCE = 1, ORACLE_POINT_VORTEX = 3 };
+/* kind of a source buffer whose rows are (x, y, z, radius, s0, s1, s2, kind): a tuple of
+ * systems concatenated in tuple order, each body carrying its own kind (1 or 3) */
+enum { ORACLE_KIND_PER_BODY = -1 };
 enum { ORACLE_LIST_SELF_TUNING_TREE_STOP = 0, ORACLE_LIST_BARBA = 1, ORACLE_LIST_SELF_TUNING = 2 };
 enum {
   ORACLE_ERR_NONE = 0,

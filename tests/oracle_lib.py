@@ -170,6 +170,30 @@ def fmm(source_buf, kind, opt, target_pos=None, want_tree=False):
         L.oracle_run_free(run)
 
 
+KIND_PER_BODY = -1
+
+
+def concat_systems(systems):
+    """A tuple of systems [(buf, kind), ...] as one (N, 8) buffer of rows
+    (x, y, z, radius, s0, s1, s2, kind), in tuple order (the oracle's tuple mode)."""
+    parts = []
+    for buf, kind in systems:
+        b = np.asarray(buf, dtype=np.float64)
+        c = np.zeros((len(b), 8))
+        c[:, :4] = b[:, :4]
+        ns = 1 if kind == POINT_SOURCE else 3
+        c[:, 4:4 + ns] = b[:, 4:4 + ns]
+        c[:, 7] = kind
+        parts.append(c)
+    return np.concatenate(parts, axis=0)
+
+
+def fmm_multi(systems, opt, target_pos, want_tree=False):
+    """The oracle fmm! on a tuple of source systems [(buf, kind), ...]: one octree over all
+    of them (Tree(systems::Tuple, ...), src/tree.jl:3-122)."""
+    return fmm(concat_systems(systems), KIND_PER_BODY, opt, target_pos=target_pos, want_tree=want_tree)
+
+
 def direct(source_buf, kind, target_pos=None, ps=1, gs=1, hs=0, n_threads=0):
     L = lib()
     sb = np.ascontiguousarray(source_buf, dtype=np.float64)

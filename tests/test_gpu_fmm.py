@@ -396,23 +396,40 @@ def test_invalid_arguments_are_errors_not_faults(ctx):
 
 
 def test_tuple_of_point_sources_and_vortices(ctx):
-    # fmm_solve_multi: one solve per kernel on the same targets, summed (the field is linear
-    # in the sources); checked bit for bit against the separate solves and, at the FMM's
-    # accuracy, against the all-pairs direct sums
+    # fmm_solve_multi: one octree over a tuple of systems (point sources and vortex
+    # particles, Tree(systems::Tuple, ...)) against the oracle's tuple mode: trees and lists
+    # bit for bit, the target buffer at 1e-10 (the potential too: with a vortex system the
+    # reference runs the Lamb-Helmholtz form, whose scalar potential it warns is not
+    # meaningful, and the restatement must reproduce it all the same)
     src = uniform(8000, 21)
     vort = ring(6000, 22)
     rng = np.random.default_rng(23)
     probes = np.ascontiguousarray(-0.5 + 2.0 * rng.random((4000, 3)))
-    og, _ = opt_pair(expansion_order=12, leaf_size_source=40, multipole_acceptance=0.4, scalar_potential=True)
-    out, res = fm.solve_multi_buffers([(src, L.FMM_POINT_SOURCE), (vort, L.FMM_POINT_VORTEX)], og, probes, ctx=ctx)
-    a, _ = fm.solve_buffers(src, L.FMM_POINT_SOURCE, og, target_pos=probes, ctx=ctx)
-    b, _ = fm.solve_buffers(vort, L.FMM_POINT_VORTEX, og, target_pos=probes, ctx=ctx)
-    np.testing.assert_array_equal(out[:, 3:], a[:, 3:] + b[:, 3:])
-    ref = O.direct(src, O.POINT_SOURCE, ps=1, gs=1, hs=0, target_pos=probes)
-    refv = O.direct(vort, O.POINT_VORTEX, ps=0, gs=1, hs=0, target_pos=probes)
-    for rows in (slice(3, 4), slice(4, 7)):
-        tot = ref[:, rows] + refv[:, rows]
-        assert rel_l2(out[:, rows], tot) < 1e-7
+    for p, em in ((12, None), (8, fm.PowerRelativeGradient(1e-7))):
+        og, oo = opt_pair(expansion_order=p, leaf_size_source=40, multipole_acceptance=0.4, scalar_potential=True,
+                          error_tolerance=em)
+        out, res = fm.solve_multi_buffers([(src, L.FMM_POINT_SOURCE), (vort, L.FMM_POINT_VORTEX)], og, probes,
+                                          ctx=ctx)
+        ref = O.fmm_multi([(src, O.POINT_SOURCE), (vort, O.POINT_VORTEX)], oo, probes, want_tree=True)
+        compare_trees(fm.get_tree(ctx, 1), ref["source_tree"])
+        compare_trees(fm.get_tree(ctx, 0), ref["target_tree"])
+        gm, gd = fm.get_lists(ctx)
+        compare_lists(gm, gd, ref["m2l"], ref["direct"])
+        assert res.p_max == ref["pmax"] and bool(res.error_success) == ref["error_success"]
+        for rows in (slice(3, 4), slice(4, 7)):
+            scale = np.abs(ref["out"][:, rows]).max()
+            np.testing.assert_allclose(out[:, rows], ref["out"][:, rows], rtol=0, atol=1e-10 * scale)
+        np.testing.assert_array_equal(out[:, :3], probes)
+        # the far field of both kernels is exercised
+        assert res.n_m2l > 0
+    # the velocity is the sum of both systems' fields, to the FMM's accuracy
+    d1 = O.direct(src, O.POINT_SOURCE, ps=1, gs=1, hs=0, target_pos=probes)
+    d3 = O.direct(vort, O.POINT_VORTEX, ps=0, gs=1, hs=0, target_pos=probes)
+    assert rel_l2(out[:, 4:7], d1[:, 4:7] + d3[:, 4:7]) < 1e-6
+    # the Barba rule splits on per-system counts: rejected, not silently different
+    ob, _ = opt_pair(expansion_order=6, leaf_size_source=40, interaction_list_method=fm.Barba())
+    with pytest.raises(fm.FMMError):
+        fm.solve_multi_buffers([(src, L.FMM_POINT_SOURCE), (vort, L.FMM_POINT_VORTEX)], ob, probes, ctx=ctx)
     # the Python fmm() on a tuple of systems of both kernels (self evaluation of the tuple)
     ps = fm.PointSources(src[:, :3], src[:, 4])
     vs = fm.VortexParticles(vort[:, :3], vort[:, 4:7])
