@@ -93,7 +93,7 @@ WORKLOADS = {
                n_cpu=20_000),
     "c5": dict(workload="serving: requests with N log-uniform [1e3, 5e5], half point sources / half vortex, uniform "
                         "cube or 8 Gaussians, PowerRelativeGradient tolerance log-uniform [1e-8, 1e-4] (p <= 16), "
-                        "Poisson arrivals at 70% of the sequential plain-FP64 capacity", n_requests=256, seed=5, workers=4,
+                        "Poisson arrivals at 70% of the sequential plain-FP64 capacity", n_requests=4096, seed=5, workers=4,
                kind=1, n=0, n_cpu=0),
     "c3": dict(workload="vortex ring N=2e6 (R=1, core sigma 0.05), p=12, leaf 80, MAC 0.4, velocity + gradient",
                n=2_000_000, gen=gen_ring, seed=3, kind=3, p=12, ls=80, mac=0.4, err=None, ps=False, gs=True,
@@ -364,8 +364,16 @@ def gpu_arm(args, w, rank, world, local_rank):
     pk = peaks()
     sm_max = pk.get("sm_max_mhz", 1965.0)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
-    fp32_peak = sms * 128 * 2 * sm_max * 1e6 / 1e12
-    fp64_peak = fp32_peak / 2
+    nominal_fp32 = sms * 128 * 2 * sm_max * 1e6 / 1e12
+    # measured CUDA-core FP32 throughput (independent FMA chains, packed and scalar): the
+    # near field's denominator; the nominal figure is kept beside it
+    meas = {}
+    for name, packed in (("packed_f32x2", 1), ("scalar", 0)):
+        v = C.c_double(0.0)
+        ctx.check(lib.fmm_measure_fp32_peak(local_rank, packed, C.byref(v)))
+        meas[name] = v.value
+    fp32_peak = max(meas.values())
+    fp64_peak = nominal_fp32 / 2
     near_flops = st_mixed["n_p2p_pairs"] * w["flops_per_pair"]
     stages = {"nearfield": st_mixed["t_nearfield_ms"], "horizontal": st_mixed["t_horizontal_ms"],
               "upward": st_mixed["t_upward_ms"], "downward": st_mixed["t_downward_ms"],
@@ -378,8 +386,9 @@ def gpu_arm(args, w, rank, world, local_rank):
         roof = {"kernel": "k_p2p (FP32, mixed)", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
                 "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": traffic,
                 "work": f"{st_mixed['n_p2p_pairs']:.3e} pairs x {w['flops_per_pair']} flop",
-                "peak_source": f"nominal FP32 CUDA-core peak, {sms} SMs x 128 lanes x 2 x {sm_max:.0f} MHz "
-                               "(MEASURED_PEAKS.json holds no CUDA-core figure)"}
+                "peak_source": "measured on this GPU in this run (fmm_measure_fp32_peak: independent FMA chains; "
+                               "MEASURED_PEAKS.json holds no CUDA-core figure)",
+                "peak_measured": meas, "peak_nominal": nominal_fp32, "frac_of_nominal": ach / nominal_fp32}
         if traffic:
             gbs = traffic / (stages["nearfield"] * 1e-3) / 1e9
             roof["hbm_view"] = {"achieved_gbs": gbs, "peak_gbs": pk.get("hbm_gbs"),
@@ -515,25 +524,31 @@ def vjp_arm(args, w):
     ctx.close()
 
 
-def serve_requests(w):
-    """The request mix of the serving workload (seeded)."""
+def serve_specs(w):
+    """The request mix of the serving workload (seeded): per request (n, kind, tolerance,
+    clustered, seed of its bodies).  Bodies are generated from the seed when the request is
+    submitted, so that 4,096 requests need not sit in host memory at once."""
     rng = np.random.default_rng(w["seed"])
-    reqs = []
+    specs = []
     for k in range(w["n_requests"]):
         n = int(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
         kind = 1 if k % 2 == 0 else 3
         tol = float(np.exp(rng.uniform(np.log(1e-8), np.log(1e-4))))
-        if rng.random() < 0.5:
-            b = gen_uniform(n, int(rng.integers(1 << 30)))
-        else:
-            b = gen_clustered(n, int(rng.integers(1 << 30)))
-        if kind == 3:
-            v = np.zeros((n, 7))
-            v[:, :4] = b[:, :4]
-            v[:, 4:7] = (2 * rng.random((n, 3)) - 1) / n
-            b = v
-        reqs.append((b, kind, tol))
-    return reqs
+        clustered = bool(rng.random() < 0.5)
+        specs.append((n, kind, tol, clustered, int(rng.integers(1 << 30))))
+    return specs
+
+
+def serve_bodies(spec):
+    n, kind, _, clustered, seed = spec
+    b = gen_clustered(n, seed) if clustered else gen_uniform(n, seed)
+    if kind == 3:
+        rng = np.random.default_rng(seed + 1)
+        v = np.zeros((n, 7))
+        v[:, :4] = b[:, :4]
+        v[:, 4:7] = (2 * rng.random((n, 3)) - 1) / n
+        b = v
+    return b
 
 
 def serve_arm(args, w):
@@ -541,14 +556,19 @@ def serve_arm(args, w):
 
     Both run the seeded request mix back to back (capacity), then replay one Poisson
     arrival stream at 70% of the sequential capacity (a rate fixed by the baseline, so
-    that latencies compare across builds); latency = completion - arrival.  Every
-    worker's buffers are grown before timing (growing frees and reallocates device
+    that latencies compare across builds); latency = completion - arrival.  The capacity
+    pass keeps a window of requests queued (the server never idles) rather than all of
+    them at once, and every request's bodies are generated just before it is submitted
+    (outside the timed intervals of the sequential passes), so host memory stays bounded.
+    Every worker's buffers are grown before timing (growing frees and reallocates device
     memory, which waits for the whole device)."""
+    import collections
     import threading
     import fastmultipole_b200 as fm
     from fastmultipole_b200 import _lib as L
-    reqs = serve_requests(w)
-    ns = np.array([len(r[0]) for r in reqs])
+    specs = serve_specs(w)
+    ns = np.array([sp[0] for sp in specs])
+    window = 64
 
     def opt_of(kind, tol):
         return fm.make_options(expansion_order=16, leaf_size_source=64 if kind == 1 else 80,
@@ -557,52 +577,65 @@ def serve_arm(args, w):
 
     def largest(limit=None):
         out = {}
-        for b, kind, tol in reqs:
-            if limit is not None and len(b) > limit:
+        for sp in specs:
+            if limit is not None and sp[0] > limit:
                 continue
-            if kind not in out or len(b) > len(out[kind][0]):
-                out[kind] = (b, kind, tol)
+            if sp[1] not in out or sp[0] > out[sp[1]][0]:
+                out[sp[1]] = sp
         return list(out.values())
 
-    def arrivals(rate):
-        return np.cumsum(np.random.default_rng(w["seed"] + 1).exponential(1.0 / rate, len(reqs)))
-
-    # sequential plain FP64 solves on one context
+    arrive = None
+    # sequential plain FP64 solves on one context (generation of the next request's bodies is
+    # excluded from the capacity time)
     seq_ctx = fm.Context(0)
-    for b, kind, tol in largest():
-        fm.solve_buffers(b, kind, opt_of(kind, tol), ctx=seq_ctx)
-    t0 = time.perf_counter()
-    for b, kind, tol in reqs:
-        fm.solve_buffers(b, kind, opt_of(kind, tol), ctx=seq_ctx)
-    seq_cap = len(reqs) / (time.perf_counter() - t0)
+    for sp in largest():
+        fm.solve_buffers(serve_bodies(sp), sp[1], opt_of(sp[1], sp[2]), ctx=seq_ctx)
+    busy = 0.0
+    for sp in specs:
+        b = serve_bodies(sp)
+        t0 = time.perf_counter()
+        fm.solve_buffers(b, sp[1], opt_of(sp[1], sp[2]), ctx=seq_ctx)
+        busy += time.perf_counter() - t0
+    seq_cap = len(specs) / busy
     rate = 0.7 * seq_cap
-    arrive = arrivals(rate)
-    seq_lat = np.zeros(len(reqs))
+    arrive = np.cumsum(np.random.default_rng(w["seed"] + 1).exponential(1.0 / rate, len(specs)))
+    # the Poisson replay: a request whose arrival has passed is solved at once
+    seq_lat = np.zeros(len(specs))
     t0 = time.perf_counter()
-    for k, (b, kind, tol) in enumerate(reqs):
+    for k, sp in enumerate(specs):
+        b = serve_bodies(sp)
         delay = t0 + arrive[k] - time.perf_counter()
         if delay > 0:
             time.sleep(delay)
-        fm.solve_buffers(b, kind, opt_of(kind, tol), ctx=seq_ctx)
+        fm.solve_buffers(b, sp[1], opt_of(sp[1], sp[2]), ctx=seq_ctx)
         seq_lat[k] = 1e3 * (time.perf_counter() - (t0 + arrive[k]))
     seq_ctx.close()
 
     ctx = fm.Context(0)
     server = fm.Server(n_workers=w["workers"], hbm_budget=150 << 30, ctx=ctx)
     n_express = max(1, w["workers"] // 2)
-    # warm-up: the general workers on the largest requests, then (while they are busy) the
-    # express workers on the largest requests they take
-    ids = [server.submit(b, kind, opt_of(kind, tol)) for b, kind, tol in largest() for _ in range(w["workers"])]
-    ids += [server.submit(b, kind, opt_of(kind, tol)) for b, kind, tol in largest(65536) for _ in range(n_express)]
+    ids = [server.submit(serve_bodies(sp), sp[1], opt_of(sp[1], sp[2])) for sp in largest()
+           for _ in range(w["workers"])]
+    ids += [server.submit(serve_bodies(sp), sp[1], opt_of(sp[1], sp[2])) for sp in largest(65536)
+            for _ in range(n_express)]
     for rid in ids:
         server.poll(rid)
-    # capacity: all requests queued at once
+    # capacity: a window of requests queued at all times; the bodies of request k + window are
+    # generated while the server works on the window
+    bodies = collections.deque(serve_bodies(sp) for sp in specs[:window])
     t0 = time.perf_counter()
-    ids = [server.submit(b, kind, opt_of(kind, tol)) for b, kind, tol in reqs]
-    for rid in ids:
-        rc, _, _ = server.poll(rid)
+    live = collections.deque()
+    nxt = 0
+    while nxt < len(specs) or live:
+        while nxt < len(specs) and len(live) < window:
+            sp = specs[nxt]
+            live.append(server.submit(bodies.popleft(), sp[1], opt_of(sp[1], sp[2])))
+            if nxt + window < len(specs):
+                bodies.append(serve_bodies(specs[nxt + window]))
+            nxt += 1
+        rc, _, _ = server.poll(live.popleft())
         assert rc == L.FMM_OK
-    cap = len(reqs) / (time.perf_counter() - t0)
+    cap = len(specs) / (time.perf_counter() - t0)
     done_at = {}
     outstanding = {}
     lock = threading.Lock()
@@ -623,16 +656,17 @@ def serve_arm(args, w):
     th = threading.Thread(target=poller)
     th.start()
     t0 = time.perf_counter()
-    for k, (b, kind, tol) in enumerate(reqs):
+    for k, sp in enumerate(specs):
+        b = serve_bodies(sp)
         delay = t0 + arrive[k] - time.perf_counter()
         if delay > 0:
             time.sleep(delay)
-        rid = server.submit(b, kind, opt_of(kind, tol))
+        rid = server.submit(b, sp[1], opt_of(sp[1], sp[2]))
         with lock:
             outstanding[rid] = k
     finished.set()
     th.join()
-    lat = np.array([1e3 * (done_at[k] - (t0 + arrive[k])) for k in range(len(reqs))])
+    lat = np.array([1e3 * (done_at[k] - (t0 + arrive[k])) for k in range(len(specs))])
     server.stop()
     ctx.close()
     line = {"metric": "serve latency p50 ms", "value": float(np.percentile(lat, 50)), "unit": "ms",
@@ -641,13 +675,13 @@ def serve_arm(args, w):
             "sequential_p99_ms": float(np.percentile(seq_lat, 99)),
             "offered_requests_per_s": rate, "capacity_requests_per_s": cap,
             "sequential_requests_per_s": seq_cap,
-            "capacity_bodies_per_s": float(ns.sum() * cap / len(reqs)),
-            "sequential_bodies_per_s": float(ns.sum() * seq_cap / len(reqs)), "capacity_vs_sequential": cap / seq_cap,
+            "capacity_bodies_per_s": float(ns.sum() * cap / len(specs)),
+            "sequential_bodies_per_s": float(ns.sum() * seq_cap / len(specs)), "capacity_vs_sequential": cap / seq_cap,
             "n_gpus": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)",
-            "config": {"workload": w["workload"], "requests": len(reqs), "workers": w["workers"],
+            "config": {"workload": w["workload"], "requests": len(specs), "workers": w["workers"],
                        "express_workers": n_express, "bodies_total": int(ns.sum()), "hbm_budget_gb": 150,
-                       "arrivals": "Poisson at 70% of the sequential capacity"}}
+                       "arrivals": "Poisson at 70% of the sequential capacity", "capacity_window": window}}
     print(json.dumps(line), flush=True)
 
 

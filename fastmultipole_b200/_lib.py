@@ -18,6 +18,8 @@ FMM_POWER_ABSOLUTE_GRADIENT = 1
 FMM_POWER_RELATIVE_GRADIENT = 2
 FMM_ROTATED_COEFFICIENTS_ABSOLUTE_GRADIENT = 3
 FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT = 4
+FMM_POWER_ABSOLUTE_POTENTIAL = 5
+FMM_POWER_RELATIVE_POTENTIAL = 6
 FMM_PRECISION_F64, FMM_PRECISION_MIXED = 0, 1
 FMM_MEMORY_HOST, FMM_MEMORY_DEVICE = 0, 1
 
@@ -98,6 +100,7 @@ SIGNATURES = {
     "fmm_serve_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Result), C.c_int]),
     "fmm_serve_stop": (C.c_int, [C.c_void_p]),
     "fmm_request_footprint": (C.c_size_t, [C.POINTER(Request)]),
+    "fmm_measure_fp32_peak": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "fmm_direct_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.POINTER(TargetSystem), C.POINTER(SourceSystem), C.c_int,
                                      C.c_int, C.c_int, C.c_int]),
     "fmm_get_tree": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TreeView)]),

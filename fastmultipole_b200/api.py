@@ -65,6 +65,14 @@ def RotatedCoefficientsRelativeGradient(eps, BE=True):
     return ErrorMethod(float(eps), bool(BE), L.FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT)
 
 
+def PowerAbsolutePotential(eps, BE=True):
+    return ErrorMethod(float(eps), bool(BE), L.FMM_POWER_ABSOLUTE_POTENTIAL)
+
+
+def PowerRelativePotential(eps, BE=True):
+    return ErrorMethod(float(eps), bool(BE), L.FMM_POWER_RELATIVE_POTENTIAL)
+
+
 @dataclass(frozen=True)
 class DerivativesSwitch:
     """DerivativesSwitch{PS,GS,HS} (src/containers.jl:50)."""

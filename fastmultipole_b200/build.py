@@ -18,7 +18,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 # comparisons bit for bit: no fused multiply-adds there
 EXACT = {"tree.cu", "lists.cu"}
 SOURCES = ["tables.cpp", "tree.cu", "lists.cu", "p2p.cu", "expansions.cu", "m2l_lane.cu", "api.cu", "noalloc.cu",
-           "serve.cpp"]
+           "serve.cpp", "peak.cu"]
 
 
 def _nvcc():

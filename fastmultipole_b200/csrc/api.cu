@@ -70,11 +70,13 @@ __global__ void k_unsort(const double* __restrict__ acc13, const int* __restrict
 
 // the influence estimate's output: |grad| of every body in the caller's order (the
 // one quantity the relative error methods read, get_influence, src/fmm.jl:1180-1183)
+// get_influence (src/fmm.jl:1180-1187) per body, caller's order: |gradient|, or the scalar
+// potential itself (potential != 0, PowerRelativePotential)
 __global__ void k_unsort_gradnorm(const double* __restrict__ acc13, const int* __restrict__ sort_index, int64_t n,
-                                  double* __restrict__ gnorm) {
+                                  double* __restrict__ gnorm, int potential = 0) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double* a = acc13 + 13 * i;
-    gnorm[sort_index ? sort_index[i] : i] = sqrt(a[1] * a[1] + a[2] * a[2] + a[3] * a[3]);
+    gnorm[sort_index ? sort_index[i] : i] = potential ? a[0] : sqrt(a[1] * a[1] + a[2] * a[2] + a[3] * a[3]);
   }
 }
 
@@ -417,8 +419,10 @@ DevTree view_tree(const DevTree& S, const SysView& v) {
   return t;
 }
 
+// is_estimate: the influence estimate's sub-solve, whose out16 receives one value per body
+// (get_influence: the scalar potential when influence_potential, else |gradient|)
 void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, double* out16, fmm_result* res,
-             bool is_estimate, cudaStream_t st, Scratch& sc, DevBuf<int>& stats) {
+             bool is_estimate, cudaStream_t st, Scratch& sc, DevBuf<int>& stats, bool influence_potential = false) {
   const int p = o.expansion_order;
   const bool multi = in.n_sys > 1;
   // lamb_helmholtz = has_vector_potential(source_systems) (src/fmm.jl:927)
@@ -500,8 +504,9 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
               o.self_induced != 0, o.list_method, o.error_method != FMM_ERROR_NONE);
   mark(2);
   FMM_CUDA_TRY(cudaMemsetAsync(T.max_influence.ptr, 0, T.n_branches * sizeof(double), st));
-  const bool estimate =
-      o.error_method == FMM_POWER_RELATIVE_GRADIENT || o.error_method == FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT;
+  const bool estimate = o.error_method == FMM_POWER_RELATIVE_GRADIENT ||
+                        o.error_method == FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT ||
+                        o.error_method == FMM_POWER_RELATIVE_POTENTIAL;
   // ---- evaluation passes (src/fmm.jl:1028-1089)
   T.local.grow(NH4 * T.n_branches);
   FMM_CUDA_TRY(cudaMemsetAsync(T.local.ptr, 0, NH4 * T.n_branches * sizeof(double), st));
@@ -520,15 +525,18 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   if (estimate || split) FMM_CUDA_TRY(cudaEventRecord(fork_event(c), st));
   if (split) FMM_CUDA_TRY(cudaStreamWaitEvent(fs, fork_event(c), 0));
   // near field
-  if (!multi) {
-    launch_p2p(T, S, W.lists, W.acc13.ptr, in.kind, ps, gs, hs, o.precision, st);
-  } else {
-    for (int k = 0; k < in.n_sys; ++k) {
-      if (W.views[k].n == 0) continue;
-      DevTree v = view_tree(S, W.views[k]);
-      launch_p2p(T, v, W.lists, W.acc13.ptr, W.views[k].kind, ps, gs, hs, o.precision, st);
+  auto near = [&] {
+    if (!multi) {
+      launch_p2p(T, S, W.lists, W.acc13.ptr, in.kind, ps, gs, hs, o.precision, st);
+    } else {
+      for (int k = 0; k < in.n_sys; ++k) {
+        if (W.views[k].n == 0) continue;
+        DevTree v = view_tree(S, W.views[k]);
+        launch_p2p(T, v, W.lists, W.acc13.ptr, W.views[k].kind, ps, gs, hs, o.precision, st);
+      }
     }
-  }
+  };
+  near();
   mark(3);
   if (o.upward_pass && !split) {
     p2m_all(st);
@@ -547,9 +555,10 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
     e.list_method = FMM_LIST_SELF_TUNING_TREE_STOP;
     e.farfield = e.nearfield = e.self_induced = 1;
     e.upward_pass = e.horizontal_pass = e.downward_pass = 1;
-    // the relative error methods read only |grad| of the estimate (get_influence,
-    // src/fmm.jl:1180-1183): its potential, which the reference also computes, is skipped
-    e.scalar_potential = 0;
+    // the relative gradient methods read only |grad| of the estimate (get_influence,
+    // src/fmm.jl:1180-1183): its potential, which the reference also computes, is skipped;
+    // PowerRelativePotential reads the potential (:1185-1187)
+    e.scalar_potential = o.error_method == FMM_POWER_RELATIVE_POTENTIAL ? 1 : 0;
     e.gradient = 1;
     e.hessian = 0;
     e.precision = o.precision;  // the mixed solve estimates with its FP32 near field
@@ -558,7 +567,8 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
     cudaStream_t es = est_stream(c);
     FMM_CUDA_TRY(cudaStreamWaitEvent(es, fork_event(c), 0));
     if (timing) FMM_CUDA_TRY(cudaEventRecord(eve[0], es));
-    run_fmm(c, c->est, in, e, c->est_out16.ptr, nullptr, true, es, est_scratch(c), est_stats(c));
+    run_fmm(c, c->est, in, e, c->est_out16.ptr, nullptr, true, es, est_scratch(c), est_stats(c),
+            o.error_method == FMM_POWER_RELATIVE_POTENTIAL);
     branch_max_influence(T, c->est_out16.ptr, es);
     if (timing) FMM_CUDA_TRY(cudaEventRecord(eve[1], es));
     FMM_CUDA_TRY(cudaEventRecord(join_event(c), es));
@@ -583,7 +593,8 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   // ---- unsort into the caller's order (buffer_to_target!, src/compatibility.jl:324-338)
   note_launch();
   if (is_estimate)  // out16 receives |grad| per body (n doubles)
-    k_unsort_gradnorm<<<grid_for(T.n_bodies), 256, 0, st>>>(W.acc13.ptr, T.sort_index.ptr, T.n_bodies, out16);
+    k_unsort_gradnorm<<<grid_for(T.n_bodies), 256, 0, st>>>(W.acc13.ptr, T.sort_index.ptr, T.n_bodies, out16,
+                                                             influence_potential ? 1 : 0);
   else
     k_unsort<<<grid_for(T.n_bodies), 256, 0, st>>>(W.acc13.ptr, T.sort_index.ptr, T.pos.ptr, T.n_bodies, out16,
                                                     split ? far13 : nullptr);
@@ -641,7 +652,7 @@ void check_options(const fmm_options& o) {
             "expansion_order must be in [1, 20]");
   FMM_CHECK(o.leaf_size_source >= 1, FMM_ERR_ARGUMENT, "leaf_size_source must be >= 1");
   FMM_CHECK(o.multipole_acceptance > 0, FMM_ERR_ARGUMENT, "multipole_acceptance must be > 0");
-  FMM_CHECK(o.error_method >= 0 && o.error_method <= 4, FMM_ERR_ARGUMENT, "unknown error_method");
+  FMM_CHECK(o.error_method >= 0 && o.error_method <= 6, FMM_ERR_ARGUMENT, "unknown error_method");
   FMM_CHECK(o.list_method >= 0 && o.list_method <= 2, FMM_ERR_ARGUMENT, "unknown list_method");
   FMM_CHECK(o.precision == FMM_PRECISION_F64 || o.precision == FMM_PRECISION_MIXED, FMM_ERR_ARGUMENT,
             "unknown precision");
@@ -1316,7 +1327,7 @@ int fmm_op_m2l(fmm_ctx* c, int64_t n, double* target, const double* tc, const do
   try {
     FMM_CHECK(p >= 1 && p <= kMaxP, FMM_ERR_ARGUMENT, "p must be in [1, 20]");
     FMM_CHECK(n >= 0 && target && tc && src && sc, FMM_ERR_ARGUMENT, "bad operator arguments");
-    FMM_CHECK(em >= 0 && em <= 4, FMM_ERR_ARGUMENT, "unknown error method");
+    FMM_CHECK(em >= 0 && em <= 6, FMM_ERR_ARGUMENT, "unknown error method");
     FMM_CUDA_TRY(cudaSetDevice(c->device));
     upload_tables(c->tables, p, c->stream);
     OpBufs B;

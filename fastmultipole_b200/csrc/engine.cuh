@@ -615,8 +615,12 @@ __device__ __forceinline__ int chain_m2l(const WS& w, double (&acc)[SLOTS][LH ? 
     rot_y_all<SLOTS, LH>(w, w.b, w.a, tb.zeta, false, L, p);
     __syncwarp();
   } else {
-    const bool relative = (em == FMM_POWER_RELATIVE_GRADIENT || em == FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT);
-    const bool power = (em == FMM_POWER_ABSOLUTE_GRADIENT || em == FMM_POWER_RELATIVE_GRADIENT);
+    const bool relative = (em == FMM_POWER_RELATIVE_GRADIENT || em == FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT ||
+                           em == FMM_POWER_RELATIVE_POTENTIAL);
+    // Power{Absolute,Relative}Potential (src/translate.jl:831-1122): the power family with
+    // the potential's error formulas
+    const bool potential = (em == FMM_POWER_ABSOLUTE_POTENTIAL || em == FMM_POWER_RELATIVE_POTENTIAL);
+    const bool power = (em == FMM_POWER_ABSOLUTE_GRADIENT || em == FMM_POWER_RELATIVE_GRADIENT || potential);
     const double eps = relative ? g.maxinf * eps_in : eps_in;
     double mdx = min_dist_1d(g.tc[0] - sc[0], -g.tbox[0], g.tbox[0]);
     double mdy = min_dist_1d(g.tc[1] - sc[1], -g.tbox[1], g.tbox[1]);
@@ -657,7 +661,10 @@ __device__ __forceinline__ int chain_m2l(const WS& w, double (&acc)[SLOTS][LH ? 
       __syncwarp();
       double eps_mp;
       const int in0 = n * (n + 1) / 2;
-      if (power) {
+      if (potential) {
+        eps_mp = 1.7320508075688772 * pn_phi * r_mp_inv_np2 * r_mp * np1_fact / (Mn0 * (n + 1));
+        if (LH) eps_mp += 1.7320508075688772 * n * pn_chi * r_mp_inv_np2 * r_mp * np1_fact / (Mn0_next * (n + 1));
+      } else if (power) {
         eps_mp = 1.7320508075688772 * mp_phi * r_mp_inv_np2 * np1_fact / Mn0;
         if (LH) eps_mp += 1.7320508075688772 * n * pn_chi * r_mp_inv_np2 * np1_fact / Mn0_next;
       } else {
@@ -696,7 +703,10 @@ __device__ __forceinline__ int chain_m2l(const WS& w, double (&acc)[SLOTS][LH ? 
           double lphi = sqrt(warp_sum_bcast(a));
           double lchi = sqrt(warp_sum_bcast(b));
           double Ln0 = tb.Lt[in0];
-          eps_l = 1.7320508075688772 * lphi * r_l_nm1 * nm1_fact_inv / Ln0;
+          if (potential)
+            eps_l = 1.7320508075688772 * lphi * r_l_nm1 * r_l * nm1_fact_inv / (Ln0 * n);
+          else
+            eps_l = 1.7320508075688772 * lphi * r_l_nm1 * nm1_fact_inv / Ln0;
           if (LH) eps_l += 1.7320508075688772 * n * lchi * r_l_nm1 * r_l * nm1_fact_inv / (Ln0 * n);
           __syncwarp();
         } else {

@@ -191,7 +191,7 @@ struct Pair {
   bool active;  // still inside the error-control loop
   bool ok;      // tolerance met
   // error control (src/translate.jl:1124-1412, :555-829)
-  double thr, r_mp_inv, r_mp_inv_np2, r_l, r_l_nm1, nm1_fact_inv, np1_fact, n_fact_t_np1, mp_phi, Mn0;
+  double thr, r_mp, r_mp_inv, r_mp_inv_np2, r_l, r_l_nm1, nm1_fact_inv, np1_fact, n_fact_t_np1, mp_phi, Mn0;
   double un;  // n! / t^(n+1) of the current degree (coaxial factor of source degree 0)
 };
 
@@ -239,8 +239,9 @@ __device__ __forceinline__ double fwd_degree(int n, const Pair& q, double* Ms, i
 // (n+j)/t in the reference's order whatever the order m, so the sums run source degrees
 // outer and orders inner (one degree's loads and FMAs independent; each sum keeps its
 // n'-ascending order).
+// power: 0 = the RotatedCoefficients methods, 1 = Power*Gradient, 2 = Power*Potential
 template <int PMAX>
-__device__ __forceinline__ double eps_local(int n, const Pair& q, const double* Ms, int lane, bool power) {
+__device__ __forceinline__ double eps_local(int n, const Pair& q, const double* Ms, int lane, int power) {
   if (power) {
     // degree n of translate_multipole_to_local_z_n! and local_power (src/translate.jl:238-295, :455-502)
     double vr[PMAX + 1], vi[PMAX + 1];
@@ -266,6 +267,8 @@ __device__ __forceinline__ double eps_local(int n, const Pair& q, const double* 
       a += (vr[m] * vr[m] + vi[m] * vi[m]) * Nt * Nt;
     }
     const double lphi = sqrt(a);
+    if (power == 2)  // src/translate.jl:912
+      return 1.7320508075688772 * lphi * q.r_l_nm1 * q.r_l * q.nm1_fact_inv / (c_Lt[hi(n, 0)] * n);
     return 1.7320508075688772 * lphi * q.r_l_nm1 * q.nm1_fact_inv / c_Lt[hi(n, 0)];
   }
   // translate_multipole_to_local_z_m01_n (src/translate.jl:302-364)
@@ -294,11 +297,13 @@ __device__ __forceinline__ double eps_local(int n, const Pair& q, const double* 
 // one degree of the reference's error-controlled loop (src/translate.jl:1124-1412,
 // :555-829) after degree n of the rotated multipole is in shared memory
 template <int PMAX>
-__device__ __forceinline__ void err_step(int n, Pair& q, const double* Ms, int lane, bool power, int be,
+__device__ __forceinline__ void err_step(int n, Pair& q, const double* Ms, int lane, int power, int be,
                                          double pn_phi, double y0r, double y1r, double y1i) {
   const double Mn0_next = c_Mt[hi(n, 0)];
   double eps_mp;
-  if (power)
+  if (power == 2)  // the potential variants read degree n's power (src/translate.jl:893)
+    eps_mp = 1.7320508075688772 * pn_phi * q.r_mp_inv_np2 * q.r_mp * q.np1_fact / (q.Mn0 * (n + 1));
+  else if (power)
     eps_mp = 1.7320508075688772 * q.mp_phi * q.r_mp_inv_np2 * q.np1_fact / q.Mn0;
   else
     eps_mp = (sqrt(y1r * y1r + y1i * y1i) + fabs(y0r)) * q.np1_fact * q.r_mp_inv_np2;
@@ -424,7 +429,7 @@ __device__ __forceinline__ double fwd_degree_f(int n, const Pair& q, float* Ms, 
 // (the coaxial sums run source degrees outer, orders inner, so that one degree's loads and
 // FMAs are independent; each sum keeps its n'-ascending order)
 template <int PMAX>
-__device__ __forceinline__ double eps_local_f(int n, const Pair& q, const float* Ms, int lane, bool power,
+__device__ __forceinline__ double eps_local_f(int n, const Pair& q, const float* Ms, int lane, int power,
                                               double tn1) {
   if (power) {
     double vr[PMAX + 1], vi[PMAX + 1];
@@ -450,6 +455,8 @@ __device__ __forceinline__ double eps_local_f(int n, const Pair& q, const float*
       a += (xr * xr + xi * xi) * Nt * Nt;
     }
     const double lphi = sqrt(a);
+    if (power == 2)
+      return 1.7320508075688772 * lphi * q.r_l_nm1 * q.r_l * q.nm1_fact_inv / (c_Lt[hi(n, 0)] * n);
     return 1.7320508075688772 * lphi * q.r_l_nm1 * q.nm1_fact_inv / c_Lt[hi(n, 0)];
   }
   double a0 = 0, b1r = 0, b1i = 0;
@@ -466,11 +473,13 @@ __device__ __forceinline__ double eps_local_f(int n, const Pair& q, const float*
 }
 
 template <int PMAX>
-__device__ __forceinline__ void err_step_f(int n, Pair& q, const float* Ms, int lane, bool power, int be,
+__device__ __forceinline__ void err_step_f(int n, Pair& q, const float* Ms, int lane, int power, int be,
                                            double pn_phi, double y0r, double y1r, double y1i, double tn1) {
   const double Mn0_next = c_Mt[hi(n, 0)];
   double eps_mp;
-  if (power)
+  if (power == 2)
+    eps_mp = 1.7320508075688772 * pn_phi * q.r_mp_inv_np2 * q.r_mp * q.np1_fact / (q.Mn0 * (n + 1));
+  else if (power)
     eps_mp = 1.7320508075688772 * q.mp_phi * q.r_mp_inv_np2 * q.np1_fact / q.Mn0;
   else
     eps_mp = (sqrt(y1r * y1r + y1i * y1i) + fabs(y0r)) * q.np1_fact * q.r_mp_inv_np2;
@@ -599,8 +608,11 @@ __global__ void __launch_bounds__(32 * W) k_m2l_lane(const int* __restrict__ tgt
   const int t = tgt_list[b];
   const double tc0 = tcen[3 * t], tc1 = tcen[3 * t + 1], tc2 = tcen[3 * t + 2];
   const bool errc = em != FMM_ERROR_NONE;
-  const bool relative = (em == FMM_POWER_RELATIVE_GRADIENT || em == FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT);
-  const bool power = (em == FMM_POWER_ABSOLUTE_GRADIENT || em == FMM_POWER_RELATIVE_GRADIENT);
+  const bool relative = (em == FMM_POWER_RELATIVE_GRADIENT || em == FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT ||
+                        em == FMM_POWER_RELATIVE_POTENTIAL);
+  const int power = (em == FMM_POWER_ABSOLUTE_POTENTIAL || em == FMM_POWER_RELATIVE_POTENTIAL)
+                        ? 2
+                        : ((em == FMM_POWER_ABSOLUTE_GRADIENT || em == FMM_POWER_RELATIVE_GRADIENT) ? 1 : 0);
   const double eps = relative ? maxinf[t] * eps_in : eps_in;
   const double tb0 = tbox[3 * t], tb1 = tbox[3 * t + 1], tb2 = tbox[3 * t + 2];
   const double r_l = trad[t];
@@ -646,6 +658,7 @@ __global__ void __launch_bounds__(32 * W) k_m2l_lane(const int* __restrict__ tgt
       if (errc) {
         const double mdx = min_dist_1d(x, -tb0, tb0), mdy = min_dist_1d(y, -tb1, tb1), mdz = min_dist_1d(z, -tb2, tb2);
         const double r_mp = sqrt(mdx * mdx + mdy * mdy + mdz * mdz);
+        q.r_mp = r_mp;
         q.r_mp_inv = 1.0 / r_mp;
         q.r_mp_inv_np2 = q.r_mp_inv * q.r_mp_inv * q.r_mp_inv;
         q.r_l = r_l;

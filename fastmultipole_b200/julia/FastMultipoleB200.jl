@@ -115,6 +115,8 @@ error_code(::PowerAbsoluteGradient{E,BE}) where {E,BE} = (Cint(1), Float64(E), C
 error_code(::PowerRelativeGradient{E,BE}) where {E,BE} = (Cint(2), Float64(E), Cint(BE))
 error_code(::RotatedCoefficientsAbsoluteGradient{E,BE}) where {E,BE} = (Cint(3), Float64(E), Cint(BE))
 error_code(::RotatedCoefficientsRelativeGradient{E,BE}) where {E,BE} = (Cint(4), Float64(E), Cint(BE))
+error_code(::FastMultipole.PowerAbsolutePotential{E,BE}) where {E,BE} = (Cint(5), Float64(E), Cint(BE))
+error_code(::FastMultipole.PowerRelativePotential{E,BE}) where {E,BE} = (Cint(6), Float64(E), Cint(BE))
 
 list_code(::SelfTuningTreeStop) = Cint(0)
 list_code(::Barba) = Cint(1)

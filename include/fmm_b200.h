@@ -66,7 +66,9 @@ typedef enum {
   FMM_POWER_ABSOLUTE_GRADIENT = 1,
   FMM_POWER_RELATIVE_GRADIENT = 2,
   FMM_ROTATED_COEFFICIENTS_ABSOLUTE_GRADIENT = 3,
-  FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT = 4
+  FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT = 4,
+  FMM_POWER_ABSOLUTE_POTENTIAL = 5, /* src/translate.jl:831-972 */
+  FMM_POWER_RELATIVE_POTENTIAL = 6  /* src/translate.jl:974-1122; influence = scalar potential */
 } fmm_error_method;
 
 /* Arithmetic of the evaluation passes. F64 is the drop-in (reference
@@ -253,6 +255,14 @@ FMM_API size_t fmm_request_footprint(const fmm_request* request);
 FMM_API int fmm_direct_noalloc(int device, void* cuda_stream, const fmm_target_system* target,
                                const fmm_source_system* source, int scalar_potential, int gradient, int hessian,
                                int precision);
+
+/* ---- measurement -----------------------------------------------------------
+ * No counterpart in the reference: the FP32 throughput of the device's CUDA cores
+ * (TFLOP/s, an FMA counting two), measured by one launch of independent fused
+ * multiply-add chains (packed != 0: f32x2 operations, the form of the mixed near
+ * field; else scalar) after a warm-up.  The roofline denominator of the near field.
+ * Allocates a 1 KB buffer; the caller's current device is restored. */
+FMM_API int fmm_measure_fp32_peak(int device, int packed, double* tflops);
 
 /* ---- parity exports of the last fmm_solve (host memory) -------------------- */
 typedef struct {

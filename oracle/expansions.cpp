@@ -750,8 +750,9 @@ static inline double min_dist_1d(double dx, double rm, double rp) {
 }
 
 // multipole_to_local! plain (src/translate.jl:519-550) and the error-controlled
-// variants RotatedCoefficients{Absolute,Relative}Gradient (:555-829) and
-// Power{Absolute,Relative}Gradient (:1124-1412).  Returns the expansion order used.
+// variants RotatedCoefficients{Absolute,Relative}Gradient (:555-829),
+// Power{Absolute,Relative}Potential (:831-1122) and Power{Absolute,Relative}Gradient
+// (:1124-1412).  Returns the expansion order used.
 int m2l(double* target, const M2LTarget& tg, const double* src, const double* sc, int p, bool lh,
         int error_method, double eps_in, int be, bool& success, Work& w) {
   const Tables& tb = tables(p);
@@ -765,8 +766,9 @@ int m2l(double* target, const M2LTarget& tg, const double* src, const double* sc
     update_Ts(w.Ts.data(), tb.Hs.data(), th, p);
     rotate_y(w.t2.data(), w.t1.data(), w.Ts.data(), tb.zeta.data(), p, lh, false);
   } else {
-    bool relative = (error_method == 2 || error_method == 4);
-    bool power = (error_method == 1 || error_method == 2);
+    bool relative = (error_method == 2 || error_method == 4 || error_method == 6);
+    bool potential = (error_method == 5 || error_method == 6);
+    bool power = (error_method == 1 || error_method == 2 || potential);
     double eps = relative ? tg.max_influence * eps_in : eps_in;
     double mdx = min_dist_1d(tg.center[0] - sc[0], -tg.box[0], tg.box[0]);
     double mdy = min_dist_1d(tg.center[1] - sc[1], -tg.box[1], tg.box[1]);
@@ -805,7 +807,11 @@ int m2l(double* target, const M2LTarget& tg, const double* src, const double* sc
       _1_n = ts_degree(w.Ts.data() + length_Ts(n - 1), tb.Hs.data() + length_Hs(n - 1), sb, cb, _1_n, n);
       rotate_y_degree(w.t2.data(), w.t1.data(), w.Ts.data(), tb.zeta.data(), n, lh, false);
       double eps_mp;
-      if (power) {
+      if (potential) {
+        // the potential variants read degree n's multipole power (src/translate.jl:893-896)
+        eps_mp = SQRT3 * pn_phi * r_mp_inv_np2 * r_mp * np1_fact / (Mn0 * (n + 1));
+        if (lh) eps_mp += SQRT3 * n * pn_chi * r_mp_inv_np2 * r_mp * np1_fact / (Mn0_next * (n + 1));
+      } else if (power) {
         eps_mp = SQRT3 * mp_phi * r_mp_inv_np2 * np1_fact / Mn0;
         if (lh) eps_mp += SQRT3 * n * pn_chi * r_mp_inv_np2 * np1_fact / Mn0_next;
       } else {
@@ -824,7 +830,10 @@ int m2l(double* target, const M2LTarget& tg, const double* src, const double* sc
           translate_multipole_to_local_z_n(w.t3.data(), w.t2.data(), rinv, n_fact_t_np1, n, lh);
           double lphi, lchi, Ln0;
           local_power(w.t3.data(), r, n, tb.Lt.data(), lh, lphi, lchi, Ln0);
-          eps_l = SQRT3 * lphi * r_l_nm1 * nm1_fact_inv / Ln0;
+          if (potential)  // src/translate.jl:912-915
+            eps_l = SQRT3 * lphi * r_l_nm1 * r_l * nm1_fact_inv / (Ln0 * n);
+          else
+            eps_l = SQRT3 * lphi * r_l_nm1 * nm1_fact_inv / Ln0;
           if (lh) eps_l += SQRT3 * n * lchi * r_l_nm1 * r_l * nm1_fact_inv / (Ln0 * n);
         } else {
           double a, b, c, d, e;

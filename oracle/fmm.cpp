@@ -573,12 +573,15 @@ static void estimate_influence(oracle_run* run, const double* target_pos, int64_
   e.hessian = 0;
   oracle_run* est = fmm_impl(target_pos, n_t, source_buf, d, kind, n_s, e, nullptr);
   if (!est) return;
+  // get_influence (src/fmm.jl:1180-1187): |gradient|, or the scalar potential itself for
+  // PowerRelativePotential
+  const bool potential = o.error_method == ORACLE_ERR_POWER_RELATIVE_POTENTIAL;
   Tree& T = run->target;
   for (auto& b : T.branches) {
     double mi = b.max_influence;
     for (int64_t i = b.body_start; i < b.body_start + b.body_count; ++i) {
-      const double* g = &est->out16[16 * T.sort_index[i] + 4];
-      mi = std::max(mi, std::sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]));
+      const double* g = &est->out16[16 * T.sort_index[i] + 3];
+      mi = std::max(mi, potential ? g[0] : std::sqrt(g[1] * g[1] + g[2] * g[2] + g[3] * g[3]));
     }
     b.max_influence = mi;
   }
@@ -630,7 +633,8 @@ static oracle_run* fmm_impl(const double* target_pos, int64_t n_t, const double*
   run->times[0] = t1 - t0;
   run->times[1] = t2 - t1;
   if (o.error_method == ORACLE_ERR_POWER_RELATIVE_GRADIENT ||
-      o.error_method == ORACLE_ERR_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT)
+      o.error_method == ORACLE_ERR_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT ||
+      o.error_method == ORACLE_ERR_POWER_RELATIVE_POTENTIAL)
     estimate_influence(run.get(), target_pos, n_t, source_buf, d, kind, n_s, o);
 
   Tree& TT = run->target;

@@ -35,7 +35,9 @@ enum {
   ORACLE_ERR_POWER_ABSOLUTE_GRADIENT = 1,
   ORACLE_ERR_POWER_RELATIVE_GRADIENT = 2,
   ORACLE_ERR_ROTATED_COEFFICIENTS_ABSOLUTE_GRADIENT = 3,
-  ORACLE_ERR_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT = 4
+  ORACLE_ERR_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT = 4,
+  ORACLE_ERR_POWER_ABSOLUTE_POTENTIAL = 5,
+  ORACLE_ERR_POWER_RELATIVE_POTENTIAL = 6
 };
 
 typedef struct {

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(ROOT, "oracle", "liboracle.so")
 POINT_SOURCE, POINT_VORTEX = 1, 3
 LIST_TREE_STOP, LIST_BARBA, LIST_SELF_TUNING = 0, 1, 2
 ERR_NONE, ERR_POWER_ABS_GRAD, ERR_POWER_REL_GRAD, ERR_ROT_ABS_GRAD, ERR_ROT_REL_GRAD = 0, 1, 2, 3, 4
+ERR_POWER_ABS_POT, ERR_POWER_REL_POT = 5, 6
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)

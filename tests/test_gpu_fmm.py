@@ -250,13 +250,15 @@ def test_mixed_vortex_far_field_matches_f64(ctx, p):
 
 
 @pytest.mark.parametrize("em", [fm.PowerRelativeGradient(1e-6), fm.PowerAbsoluteGradient(1e-4),
-                                fm.RotatedCoefficientsRelativeGradient(1e-6)], ids=["prg", "pag", "rcrg"])
+                                fm.RotatedCoefficientsRelativeGradient(1e-6), fm.PowerAbsolutePotential(1e-3),
+                                fm.PowerRelativePotential(1e-6)], ids=["prg", "pag", "rcrg", "pap", "prp"])
 def test_error_controlled_orders_match_oracle(ctx, em):
     buf = clustered(15000, 5)
     og, oo = opt_pair(expansion_order=10, leaf_size_source=64, multipole_acceptance=0.5, error_tolerance=em)
     out, res = fm.solve_buffers(buf, L.FMM_POINT_SOURCE, og, ctx=ctx)
     ref = O.fmm(buf, O.POINT_SOURCE, oo, want_tree=True)
-    if em.code in (L.FMM_POWER_RELATIVE_GRADIENT, L.FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT):
+    if em.code in (L.FMM_POWER_RELATIVE_GRADIENT, L.FMM_ROTATED_COEFFICIENTS_RELATIVE_GRADIENT,
+                   L.FMM_POWER_RELATIVE_POTENTIAL):
         g = fm.get_tree(ctx, 0)
         np.testing.assert_allclose(g["max_influence"], ref["target_tree"]["max_influence"], rtol=1e-11, atol=0)
     assert res.p_max == ref["pmax"]

@@ -138,7 +138,8 @@ def test_golden_vorton_p2m_m2l_l2p(ctx):
 
 
 @pytest.mark.parametrize("p,lh,em", [(6, 0, 0), (10, 0, 0), (12, 1, 0), (16, 0, 0), (10, 0, 1), (10, 0, 2),
-                                     (10, 1, 2), (10, 0, 3), (12, 1, 4), (20, 0, 0)])
+                                     (10, 1, 2), (10, 0, 3), (12, 1, 4), (20, 0, 0), (10, 0, 5), (10, 1, 6),
+                                     (14, 0, 6)])
 def test_m2l_batch_matches_oracle(ctx, p, lh, em):
     rng = np.random.default_rng(100 * p + 10 * lh + em)
     n = 64
