@@ -432,7 +432,9 @@ def gpu_arm(args, w, rank, world, local_rank):
 
 def vjp_arm(args, w):
     """Adjoint workload: one step = forward solve at the probes (phi), then fmm_vjp with
-    dL/dphi = 2 phi (L = sum phi^2); device-resident inputs; CUDA-event timing."""
+    dL/dphi = 2 phi (L = sum phi^2); device-resident inputs; CUDA-event timing.  Both
+    precisions are timed (value: the FP64 drop-in) and both gradients are checked by central
+    finite differences of the exact loss (FP64 all-pairs) on the same 64 coordinates."""
     import torch
     import fastmultipole_b200 as fm
     from fastmultipole_b200 import _lib as L
@@ -453,29 +455,34 @@ def vjp_arm(args, w):
     dy = torch.empty((npr, 3), dtype=torch.float64, device=dev)
     src = L.SourceSystem(1, n, 5, src_dev.data_ptr(), L.FMM_MEMORY_DEVICE)
     tgt = L.TargetSystem(npr, pr_dev.data_ptr(), 3, out_dev.data_ptr(), L.FMM_MEMORY_DEVICE)
-    opt = fm.make_options(expansion_order=w["p"], leaf_size_source=w["ls"], multipole_acceptance=w["mac"],
-                          scalar_potential=True, gradient=True)
     res = L.Result()
     dp = L._dp
 
-    def step():
-        ctx.check(lib.fmm_solve(ctx.handle, C.byref(tgt), C.byref(src), C.byref(opt), C.byref(res)))
-        dout[:, 3] = 2.0 * out_dev[:, 3]
-        ctx.check(lib.fmm_vjp(ctx.handle, C.byref(tgt), C.byref(src), C.byref(opt),
-                              C.cast(dout.data_ptr(), dp), C.cast(dq.data_ptr(), dp), C.cast(dx.data_ptr(), dp),
-                              C.cast(dy.data_ptr(), dp), C.byref(res)))
+    def run(precision):
+        opt = fm.make_options(expansion_order=w["p"], leaf_size_source=w["ls"], multipole_acceptance=w["mac"],
+                              scalar_potential=True, gradient=True, precision=precision)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    e1.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    # central finite differences of the exact loss (all-pairs direct) on 16 coordinates
+        def step():
+            ctx.check(lib.fmm_solve(ctx.handle, C.byref(tgt), C.byref(src), C.byref(opt), C.byref(res)))
+            dout[:, 3] = 2.0 * out_dev[:, 3]
+            ctx.check(lib.fmm_vjp(ctx.handle, C.byref(tgt), C.byref(src), C.byref(opt),
+                                  C.cast(dout.data_ptr(), dp), C.cast(dq.data_ptr(), dp),
+                                  C.cast(dx.data_ptr(), dp), C.cast(dy.data_ptr(), dp), C.byref(res)))
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / args.steps, dq.cpu().numpy(), dx.cpu().numpy(), dy.cpu().numpy()
+
+    ms, gq, gx, gy = run("f64")
+    ms_mx, gq_mx, gx_mx, gy_mx = run("mixed")
+    # central finite differences of the exact loss (all-pairs direct) on 64 coordinates
     phi = np.zeros((npr, 16))
 
     def loss(b, pr):
@@ -486,11 +493,10 @@ def vjp_arm(args, w):
         ctx.check(lib.fmm_direct(ctx.handle, C.byref(t_), C.byref(s_), 1, 0, 0, L.FMM_PRECISION_F64))
         return float(np.sum(phi[:, 3] ** 2))
 
-    gq, gx, gy = dq.cpu().numpy(), dx.cpu().numpy(), dy.cpu().numpy()
     rng = np.random.default_rng(9)
-    errs = []
+    errs, errs_mx = [], []
     h = 1e-6
-    for _ in range(16):
+    for _ in range(64):
         which = rng.integers(0, 3)
         if which == 0:
             i = rng.integers(0, n)
@@ -500,6 +506,7 @@ def vjp_arm(args, w):
             bm[i, 4] -= hq
             fd = (loss(bp, probes) - loss(bm, probes)) / (2 * hq)
             errs.append(abs(gq[i] - fd) / np.abs(gq).max())
+            errs_mx.append(abs(gq_mx[i] - fd) / np.abs(gq).max())
         elif which == 1:
             i, k = rng.integers(0, n), rng.integers(0, 3)
             bp, bm = buf.copy(), buf.copy()
@@ -507,6 +514,7 @@ def vjp_arm(args, w):
             bm[i, k] -= h
             fd = (loss(bp, probes) - loss(bm, probes)) / (2 * h)
             errs.append(abs(gx[i, k] - fd) / np.abs(gx).max())
+            errs_mx.append(abs(gx_mx[i, k] - fd) / np.abs(gx).max())
         else:
             i, k = rng.integers(0, npr), rng.integers(0, 3)
             pp, pm = probes.copy(), probes.copy()
@@ -514,12 +522,14 @@ def vjp_arm(args, w):
             pm[i, k] -= h
             fd = (loss(buf, pp) - loss(buf, pm)) / (2 * h)
             errs.append(abs(gy[i, k] - fd) / np.abs(gy).max())
+            errs_mx.append(abs(gy_mx[i, k] - fd) / np.abs(gy).max())
     line = {"metric": "FMM loss gradient (forward + adjoint) sources/s", "value": n / (ms * 1e-3),
             "unit": "sources/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)",
             "config": {"workload": w["workload"], "n_sources": n, "n_probes": npr, "solves_per_step": 3},
-            "fd_max_rel_dev": float(max(errs)), "fd_coordinates": 16}
+            "fd_max_rel_dev": float(max(errs)), "fd_coordinates": len(errs),
+            "mixed": {"value": n / (ms_mx * 1e-3), "ms_per_step": ms_mx, "fd_max_rel_dev": float(max(errs_mx))}}
     print(json.dumps(line), flush=True)
     ctx.close()
 

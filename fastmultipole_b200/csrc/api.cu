@@ -527,12 +527,12 @@ void run_fmm(fmm_ctx* c, Workspace& W, const SolveIn& in, const fmm_options& o, 
   // near field
   auto near = [&] {
     if (!multi) {
-      launch_p2p(T, S, W.lists, W.acc13.ptr, in.kind, ps, gs, hs, o.precision, st);
+      launch_p2p(T, S, W.lists, W.acc13.ptr, in.kind, ps, gs, hs, o.precision, st, !is_estimate);
     } else {
       for (int k = 0; k < in.n_sys; ++k) {
         if (W.views[k].n == 0) continue;
         DevTree v = view_tree(S, W.views[k]);
-        launch_p2p(T, v, W.lists, W.acc13.ptr, W.views[k].kind, ps, gs, hs, o.precision, st);
+        launch_p2p(T, v, W.lists, W.acc13.ptr, W.views[k].kind, ps, gs, hs, o.precision, st, !is_estimate);
       }
     }
   };

@@ -107,8 +107,9 @@ void export_lists_reference_order(const DevLists& L, const DevTree& tt, const De
 
 // ---- p2p.cu ----
 // Near field over the direct list; accumulates into acc13 (sorted target order, 13 per body).
+// exact_self: on the mixed path, evaluate the batch holding the target's own leaf in FP64
 void launch_p2p(const DevTree& tt, const DevTree& stt, DevLists& L, double* acc13, int kind, bool ps,
-                bool gs, bool hs, int precision, cudaStream_t st);
+                bool gs, bool hs, int precision, cudaStream_t st, bool exact_self = true);
 // sum over the direct list of n_target * n_source (atomically added to *out)
 void count_p2p_pairs(const DevTree& tt, const DevTree& stt, const DevLists& L, unsigned long long* out,
                      cudaStream_t st);

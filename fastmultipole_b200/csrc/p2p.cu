@@ -259,9 +259,11 @@ __device__ __forceinline__ void packed_batch(const float4* __restrict__ B4, int 
     } else {
       ri = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
     }
+    // q / r and q / r^3 = (q / r) (1 / r^2): the two products after the rsqrt are independent
     const float2 qr = __fmul2_rn(make_float2(v.z, v.w), ri);
+    const float2 ri2 = __fmul2_rn(ri, ri);
     if (PS) ph = __fadd2_rn(ph, qr);
-    const float2 q3 = __fmul2_rn(__fmul2_rn(qr, ri), ri);
+    const float2 q3 = __fmul2_rn(qr, ri2);
     gx = __ffma2_rn(dx, q3, gx);
     gy = __ffma2_rn(dy, q3, gy);
     gz = __ffma2_rn(dz, q3, gz);
@@ -492,7 +494,8 @@ __global__ void __launch_bounds__(W * 32, p2p_min_blocks<R, KIND, HS, RW, W>()) 
                                                      const int* __restrict__ s_start, const int* __restrict__ s_count,
                                                      const double4* __restrict__ tpos, const double4* __restrict__ spos,
                                                      const double4* __restrict__ sstr, double* __restrict__ acc13,
-                                                     const int4* __restrict__ chunks, double* __restrict__ chunk_sums) {
+                                                     const int4* __restrict__ chunks, double* __restrict__ chunk_sums,
+                                                     int exact_self) {
   // chunks (CTA path only; may be null): CTA b takes the source leaves [y, z) of row x and stores
   // its sums (unscaled, not atomically) at chunk_sums + w + NA * (target index in the row) + channel
   constexpr int NB = batch_bodies<R, KIND>(), NV = Batch<KIND>::nv, NA = n_chan<KIND, GS, HS>();
@@ -584,6 +587,9 @@ __global__ void __launch_bounds__(W * 32, p2p_min_blocks<R, KIND, HS, RW, W>()) 
       }
       // the batch holds the target branch's own bodies (coincident pairs certain)
       const bool self_batch = __any_sync(kAll, lane < nl && sl == t);
+      // mixed path: that batch in FP64 (the solve's own near field; the influence estimate, which
+      // only needs the magnitude of the field, keeps it in FP32 with the r^2 > 0 guard)
+      const bool self_f64 = self_batch && exact_self != 0;
       // gather: body idx of the batch lies in candidate leaf k (largest k < nl with excl_k <= idx)
       for (int i0 = 0; i0 < nb; i0 += 32) {
         const int idx = i0 + lane;
@@ -596,7 +602,7 @@ __global__ void __launch_bounds__(W * 32, p2p_min_blocks<R, KIND, HS, RW, W>()) 
         }
         const int ek = __shfl_sync(kAll, excl, k);
         const int sk = __shfl_sync(kAll, sb, k);
-        if ((PACK || PACKV) && self_batch && idx < nb) {
+        if ((PACK || PACKV) && self_f64 && idx < nb) {
           // FP64 (x, y, z, q) / (x, y, z, G0), (G1, G2, -, -) relative to the target leaf centre
           const int body = sk + idx - ek;
           const double4 p = spos[body];
@@ -651,10 +657,12 @@ __global__ void __launch_bounds__(W * 32, p2p_min_blocks<R, KIND, HS, RW, W>()) 
         // the batch holding the target's own leaf runs in FP64 and skips coincident bodies;
         // the others run unguarded and, in the rare case that their sums come out non-finite
         // (bodies that coincide in FP32), repeat the batch with the r^2 > 0 guard
-        if (self_batch) {
+        if (self_f64) {
           double txd[2], tyd[2], tzd[2];
           self_targets_f64(tpos, ts + tile, nt, ti, TS, ox, oy, oz, txd, tyd, tzd);
           self_batch_f64_source<PS, NA>(reinterpret_cast<const double4*>(B), slice, nb, SS, txd, tyd, tzd, tot);
+        } else if (self_batch) {
+          packed_batch<true, PS>(B4, slice, nb, SS, tx2, ty2, tz2, ph, gx, gy, gz);
         } else {
           packed_batch<false, PS>(B4, slice, nb, SS, tx2, ty2, tz2, ph, gx, gy, gz);
           if (!isfinite(ph.x + ph.y + gx.x + gx.y + gy.x + gy.y + gz.x + gz.y)) {
@@ -677,12 +685,14 @@ __global__ void __launch_bounds__(W * 32, p2p_min_blocks<R, KIND, HS, RW, W>()) 
         const float4* B4 = reinterpret_cast<const float4*>(B);
         float2 acc[NA];
         // as on the point-source path: the batch holding the target's own leaf runs in FP64
-        if (self_batch) {
+        if (self_f64) {
 #pragma unroll
           for (int a = 0; a < NA; ++a) acc[a] = make_float2(0.f, 0.f);
           double txd[2], tyd[2], tzd[2];
           self_targets_f64(tpos, ts + tile, nt, ti, TS, ox, oy, oz, txd, tyd, tzd);
           self_batch_f64_vortex<GS, HS, NA>(reinterpret_cast<const double2*>(B), slice, nb, SS, txd, tyd, tzd, tot);
+        } else if (self_batch) {
+          packed_vortex_batch<true, GS, HS, NA>(B4, slice, nb, SS, tx2, ty2, tz2, acc);
         } else {
           packed_vortex_batch<false, GS, HS, NA>(B4, slice, nb, SS, tx2, ty2, tz2, acc);
           float sum = 0.f;
@@ -866,7 +876,7 @@ __global__ void k_p2p_chunk_sum(const int4* __restrict__ rowtab, const int4* __r
 }
 
 template <class R, int KIND, bool PS, bool GS, bool HS>
-void run_p2p(const DevTree& tt, const DevTree& stt, DevLists& L, double* acc13, cudaStream_t st) {
+void run_p2p(const DevTree& tt, const DevTree& stt, DevLists& L, double* acc13, int exact_self, cudaStream_t st) {
   if (L.n_dir_targets == 0) return;
   constexpr size_t smem = p2p_smem_bytes<R, KIND, GS, HS>();
   const int rows = (int)L.n_dir_targets;
@@ -880,7 +890,7 @@ void run_p2p(const DevTree& tt, const DevTree& stt, DevLists& L, double* acc13, 
     k_p2p<R, KIND, PS, GS, HS, true><<<(rows + kWarps - 1) / kWarps, kWarps * 32, smem, st>>>(
         L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
         stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13, nullptr,
-        nullptr);
+        nullptr, exact_self);
   } else {
     int dev = 0, n_sm = 0;
     FMM_CUDA_TRY(cudaGetDevice(&dev));
@@ -897,7 +907,8 @@ void run_p2p(const DevTree& tt, const DevTree& stt, DevLists& L, double* acc13, 
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw));
       k_p2p<R, KIND, PS, GS, HS, false, kWideWarps><<<rows, kWideWarps * 32, smw, st>>>(
           L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
-          stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13, nullptr, nullptr);
+          stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13, nullptr, nullptr,
+          exact_self);
     } else if (rows < kWideRowsPerSM * n_sm) {
       // few rows: cut them into chunks of about the same number of source leaves (some
       // kChunksPerSM per SM over the launch), one wide CTA each; the chunks' partial sums are
@@ -937,7 +948,7 @@ void run_p2p(const DevTree& tt, const DevTree& stt, DevLists& L, double* acc13, 
       k_p2p<R, KIND, PS, GS, HS, false, kWideWarps><<<(int)ch.size(), kWideWarps * 32, smw, st>>>(
           L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
           stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13, L.p2p_chunks.ptr,
-          L.p2p_part.ptr);
+          L.p2p_part.ptr, exact_self);
       FMM_CUDA_TRY(cudaGetLastError());
       note_launch();
       k_p2p_chunk_sum<KIND, PS, GS, NA><<<rows, 256, 0, st>>>(L.p2p_rowtab.ptr, L.p2p_chunks.ptr, L.p2p_part.ptr,
@@ -950,7 +961,7 @@ void run_p2p(const DevTree& tt, const DevTree& stt, DevLists& L, double* acc13, 
       k_p2p<R, KIND, PS, GS, HS, false><<<rows, kWarps * 32, smem, st>>>(
           L.dir_tgt.ptr, L.dir_off.ptr, rows, L.dir_s.ptr, tt.body_start.ptr, tt.body_count.ptr, tt.tcenter.ptr,
           stt.body_start.ptr, stt.body_count.ptr, tt.pos.ptr, stt.pos.ptr, stt.str.ptr, acc13, nullptr,
-        nullptr);
+        nullptr, exact_self);
     }
   }
   FMM_CUDA_TRY(cudaGetLastError());
@@ -990,10 +1001,11 @@ struct P2PLaunch {
   const DevTree& stt;
   DevLists& L;
   double* acc13;
+  int exact_self;
   cudaStream_t st;
   template <class R, int K, bool PS, bool GS, bool HS>
   void go() {
-    run_p2p<R, K, PS, GS, HS>(tt, stt, L, acc13, st);
+    run_p2p<R, K, PS, GS, HS>(tt, stt, L, acc13, exact_self, st);
   }
 };
 
@@ -1033,8 +1045,8 @@ void count_p2p_pairs(const DevTree& tt, const DevTree& stt, const DevLists& L, u
 }
 
 void launch_p2p(const DevTree& tt, const DevTree& stt, DevLists& L, double* acc13, int kind, bool ps, bool gs,
-                bool hs, int precision, cudaStream_t st) {
-  P2PLaunch f{tt, stt, L, acc13, st};
+                bool hs, int precision, cudaStream_t st, bool exact_self) {
+  P2PLaunch f{tt, stt, L, acc13, exact_self ? 1 : 0, st};
   if (precision == FMM_PRECISION_MIXED)
     dispatch<float>(kind, ps, gs, hs, f);
   else

@@ -180,6 +180,46 @@ end
 fmm!(system; leaf_size=20, kwargs...) = fmm!(system, system; leaf_size_source=leaf_size, kwargs...)
 
 """
+    fmm!(target_system, source_systems::Tuple; kwargs...)
+
+A tuple of source systems (point sources and vortex particles mixed): one octree over
+the bodies of all of them, as `Tree(systems::Tuple, ...)` builds it (src/tree.jl:3-122),
+through `fmm_solve_multi`.  The target system gets the summed field.
+"""
+function fmm!(target_system, source_systems::Tuple; expansion_order=5, leaf_size_source=20, leaf_size_target=nothing,
+              multipole_acceptance=0.4, error_tolerance=nothing, shrink_recenter=true,
+              interaction_list_method=SelfTuningTreeStop(), scalar_potential=false, gradient=true, hessian=false,
+              farfield=true, nearfield=true, self_induced=true, upward_pass=true, horizontal_pass=true,
+              downward_pass=true, precision=:f64)
+    length(source_systems) == 1 && return fmm!(target_system, source_systems[1]; expansion_order, leaf_size_source,
+        leaf_size_target, multipole_acceptance, error_tolerance, shrink_recenter, interaction_list_method,
+        scalar_potential, gradient, hessian, farfield, nearfield, self_induced, upward_pass, horizontal_pass,
+        downward_pass, precision)
+    bufs = [source_buffer(s) for s in source_systems]
+    n_t = get_n_bodies(target_system)
+    pos = reduce(hcat, [Vector{Float64}(get_position(target_system, i)) for i in 1:n_t])
+    out = zeros(Float64, 16, n_t)
+    em, eps, be = error_code(error_tolerance)
+    opt = FmmOptions(expansion_order, leaf_size_source, something(leaf_size_target, 0), multipole_acceptance,
+                     em, eps, be, shrink_recenter, list_code(interaction_list_method), farfield, nearfield,
+                     self_induced, upward_pass, horizontal_pass, downward_pass, scalar_potential, gradient, hessian,
+                     precision == :mixed ? 1 : 0)
+    res = FmmResult()
+    GC.@preserve bufs pos out begin
+        srcs = [FmmSourceSystem(kernel_kind(s), size(b, 2), size(b, 1), pointer(b), 0)
+                for (s, b) in zip(source_systems, bufs)]
+        tgt = FmmTargetSystem(n_t, pointer(pos), 3, pointer(out), 0)
+        check(ccall((:fmm_solve_multi, libfmm), Cint,
+                    (Ptr{Cvoid}, Ref{FmmTargetSystem}, Ptr{FmmSourceSystem}, Cint, Ref{FmmOptions}, Ref{FmmResult}),
+                    context(), tgt, srcs, length(srcs), opt, res))
+    end
+    scatter!(target_system, out, DerivativesSwitch(scalar_potential, gradient, hessian))
+    optimized_args = (leaf_size_source=leaf_size_source, expansion_order=max(expansion_order, 1),
+                      multipole_acceptance=multipole_acceptance)
+    return optimized_args, res, res.error_success != 0
+end
+
+"""
     direct!(target_system, source_system; scalar_potential=false, gradient=true, hessian=false)
 
 FastMultipole.direct! (src/direct.jl:20-75) on the B200, all pairs.

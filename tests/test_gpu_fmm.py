@@ -437,3 +437,34 @@ def test_tuple_of_point_sources_and_vortices(ctx):
     vs = fm.VortexParticles(vort[:, :3], vort[:, 4:7])
     fm.fmm((ps, vs), expansion_order=8, leaf_size=40, multipole_acceptance=0.5, context=ctx)
     assert np.isfinite(ps.potential).all() and np.isfinite(vs.potential).all()
+
+
+def test_tuple_edge_cases(ctx):
+    # a tuple of two point-source systems is the concatenation of their bodies (one octree,
+    # systems one after another inside each leaf): the single-system solve of the concatenated
+    # buffer to rounding (per-system P2M and P2P batches sum in another order); an empty system
+    # in a tuple changes nothing; three systems agree with the oracle's tuple mode
+    a = uniform(5000, 31)
+    b = uniform(4000, 32)
+    v = ring(3000, 33)
+    rng = np.random.default_rng(34)
+    probes = np.ascontiguousarray(rng.random((2500, 3)))
+    og, oo = opt_pair(expansion_order=7, leaf_size_source=30, multipole_acceptance=0.5, scalar_potential=True)
+    out2, _ = fm.solve_multi_buffers([(a, L.FMM_POINT_SOURCE), (b, L.FMM_POINT_SOURCE)], og, probes, ctx=ctx)
+    cat, _ = fm.solve_buffers(np.concatenate([a, b]), L.FMM_POINT_SOURCE, og, target_pos=probes, ctx=ctx)
+    np.testing.assert_array_equal(out2[:, :3], cat[:, :3])
+    np.testing.assert_allclose(out2[:, 3:7], cat[:, 3:7], rtol=0, atol=1e-12 * np.abs(cat[:, 3:7]).max())
+    empty = np.zeros((0, 7))
+    out3, _ = fm.solve_multi_buffers([(a, L.FMM_POINT_SOURCE), (empty, L.FMM_POINT_VORTEX), (v, L.FMM_POINT_VORTEX)],
+                                     og, probes, ctx=ctx)
+    out3b, _ = fm.solve_multi_buffers([(a, L.FMM_POINT_SOURCE), (v, L.FMM_POINT_VORTEX)], og, probes, ctx=ctx)
+    np.testing.assert_array_equal(out3, out3b)
+    out4, res = fm.solve_multi_buffers([(a, L.FMM_POINT_SOURCE), (v, L.FMM_POINT_VORTEX), (b, L.FMM_POINT_SOURCE)],
+                                       og, probes, ctx=ctx)
+    ref = O.fmm_multi([(a, O.POINT_SOURCE), (v, O.POINT_VORTEX), (b, O.POINT_SOURCE)], oo, probes, want_tree=True)
+    compare_trees(fm.get_tree(ctx, 1), ref["source_tree"])
+    gm, gd = fm.get_lists(ctx)
+    compare_lists(gm, gd, ref["m2l"], ref["direct"])
+    for rows in (slice(3, 4), slice(4, 7)):
+        scale = np.abs(ref["out"][:, rows]).max()
+        np.testing.assert_allclose(out4[:, rows], ref["out"][:, rows], rtol=0, atol=1e-10 * scale)

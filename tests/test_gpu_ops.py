@@ -218,3 +218,12 @@ def test_l2p_matches_oracle(ctx, p, lh):
         O.lib().oracle_l2p(O.dptr(dx[k].copy()), O.dptr(Lx), p, lh, 1, 1, 1, O.dptr(phi), O.dptr(g), O.dptr(H))
         ref = np.concatenate([phi, g, H])
         np.testing.assert_allclose(out[k], ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+
+
+def test_measured_fp32_peak_is_plausible():
+    # the near field's roofline denominator: independent FMA chains on every SM of a B200
+    # (nominal 148 SMs x 128 lanes x 2 flop x ~1.9 GHz = 74 TFLOP/s)
+    for packed in (0, 1):
+        v = C.c_double(0.0)
+        assert L.lib().fmm_measure_fp32_peak(0, packed, C.byref(v)) == L.FMM_OK
+        assert 20.0 < v.value < 90.0, (packed, v.value)
