@@ -116,7 +116,9 @@ void ensure_lane_tables(cudaStream_t st) {
 // loop runs at run time and fuses both matrix products: column nu of B H gives
 // E, O, Z, and P_nu +- Q_nu is accumulated into every output at once through
 // column nu of A H w / 2.  Sums run to PMAX from one column base, so the table
-// entries are uniform constant reads at fixed offsets and no term is predicated.
+// entries are uniform constant reads at fixed offsets and no term is predicated
+// (measured: sums that stop at the degree are slower, the fixed trip counts
+// schedule better than the skipped terms save).
 template <bool LOCAL, class V>
 __device__ __forceinline__ V tab_b(int i) {
   if constexpr (sizeof(V) == 8)
@@ -1294,32 +1296,32 @@ struct L2LLaneGo {
 };
 
 // ---- Lamb-Helmholtz (vortex particle) plain M2L ---------------------------------
-// One warp per target branch, one lane per (target, source) pair, as k_m2l_lane.  The two
-// expansion sets (phi: 0, chi: 1) share every rotation.  Before the rotations (in V: FP32 on the
-// mixed path, FP64 on the drop-in path) set 0 of
-// the multipole is scaled by t^-n and set 1 by t^(1-n); the coaxial translation with (n+n')!
-// then gives the local sets times t^(n+1) and t^(n+2), on which the Lamb-Helmholtz coupling
-// of transform_lamb_helmholtz_local! (src/translate.jl:98-142) needs no power of t:
+// One warp per target branch, two lanes per (target, source) pair: lanes 0-15 carry set 0
+// (phi) and lanes 16-31 set 1 (chi) of the same 16 pairs, so each lane rotates, translates
+// and rotates back one set.  Before the rotations (in V: FP32 on the mixed path, FP64 on the
+// drop-in path) set 0 of the multipole is scaled by t^-n and set 1 by t^(1-n); the coaxial
+// translation with (n+n')! then gives the local sets times t^(n+1) and t^(n+2), on which the
+// Lamb-Helmholtz coupling of transform_lamb_helmholtz_local! (src/translate.jl:98-142) needs no
+// power of t:
 //   phi(n, m) -= i (m / n) chi(n, m),  chi(n, m) -= chi(n + 1, m) / (n + 1).
-// The rotated-back degrees are staged in shared memory unscaled (in V) with each lane's
-// t^-(n+1) / t^-(n+2), and summed over the lanes in FP64, value times power, into the warp's
-// FP64 accumulator: an FP32 stage keeps the warp's shared memory at order 12 to 55.5 KB
-// (4 CTAs per SM instead of 3 with an FP64 stage).
-template <class V>
-__device__ __forceinline__ V& MSl(V* Ms, int i, int c, int lane) { return Ms[(4 * i + c) * 32 + lane]; }
-
+// The chi lane translates one degree ahead (it needs chi(n + 1)) and keeps chi(n) from the
+// step before, which the phi lane reads across the warp (xor 16).  The rotated-back degrees are
+// staged in shared memory unscaled (in V) with each lane's t^-(n+1) (phi) or t^-(n+2) (chi),
+// and summed over the 16 pairs in FP64, value times power, into the warp's FP64 accumulator.
+// One set per lane halves the registers and the shared memory a pair holds on a lane
+// (order 12, FP32: 30 KB per warp, 7 warps per SM instead of 4 with a pair per lane).
 template <int PMAX, class V>
 constexpr size_t lane_lh_smem_bytes() {
-  return ((size_t)4 * hi(PMAX + 1, 0) + 64) * sizeof(double) +
-         ((size_t)4 * (PMAX + 1) * 33 + (size_t)4 * hi(PMAX + 1, 0) * 32) * sizeof(V);
+  return ((size_t)4 * hi(PMAX + 1, 0) + 32) * sizeof(double) +
+         ((size_t)4 * (PMAX + 1) * 17 + (size_t)2 * hi(PMAX + 1, 0) * 32) * sizeof(V);
 }
 
-// coaxial translation of one set (c0 = 0 or 2) of degree n, scaled: sum_{n'} (n+n')! M(n', m)
+// coaxial translation of the lane's set, degree n, orders m <= mmax, scaled:
+// sum_{n'} (n+n')! M(n', m) (source degrees outer, orders inner: one degree's loads and FMAs
+// are independent, each sum keeps its n'-ascending order)
 template <int PMAX, class V>
-__device__ __forceinline__ void coax_lh(int n, int P, const V* Ms, int c0, int lane, V (&Xr)[PMAX + 1],
+__device__ __forceinline__ void coax_lh(int n, int mmax, int P, const V* Ms, int lane, V (&Xr)[PMAX + 1],
                                         V (&Xi)[PMAX + 1]) {
-  // source degrees outer, orders inner: one degree's loads and FMAs are independent (each
-  // sum keeps its n'-ascending order)
 #pragma unroll
   for (int m = 0; m <= PMAX; ++m) Xr[m] = Xi[m] = V(0);
 #pragma unroll 2
@@ -1328,9 +1330,9 @@ __device__ __forceinline__ void coax_lh(int n, int P, const V* Ms, int c0, int l
     const int base = hi(np, 0);
 #pragma unroll
     for (int m = 0; m <= PMAX; ++m) {
-      if (m > n || m > np) break;
-      Xr[m] += c * Ms[(4 * (base + m) + c0) * 32 + lane];
-      Xi[m] += c * Ms[(4 * (base + m) + c0 + 1) * 32 + lane];
+      if (m > mmax || m > np) break;
+      Xr[m] += c * Ms[(2 * (base + m)) * 32 + lane];
+      Xi[m] += c * Ms[(2 * (base + m) + 1) * 32 + lane];
     }
   }
 }
@@ -1345,26 +1347,27 @@ __global__ void __launch_bounds__(32) k_m2l_lane_lh(const int* __restrict__ tgt_
   constexpr int NH = hi(PMAX + 1, 0);
   extern __shared__ double lane_smem[];
   double* acc = lane_smem;                    // [4 NH]
-  double* tsc = acc + 4 * NH;                 // per lane t^-(n+1), t^-(n+2): [2][32]
-  V* stage = reinterpret_cast<V*>(tsc + 64);  // unscaled rotated-back values [4 (PMAX+1)][33]
-  V* Ms = stage + 4 * (PMAX + 1) * 33;        // rotated multipole [4 NH][32]
+  double* tsc = acc + 4 * NH;                 // per pair t^-(n+1) (set 0), t^-(n+2) (set 1): [2][16]
+  V* stage = reinterpret_cast<V*>(tsc + 32);  // unscaled rotated-back values [4 (PMAX+1)][17]
+  V* Ms = stage + 4 * (PMAX + 1) * 17;        // rotated multipole of the lane's set [2 NH][32]
   const int lane = threadIdx.x;
+  const int set = lane >> 4, slot = lane & 15;
   const int b = blockIdx.x;
   const int t = tgt_list[b];
   const double tc0 = tcen[3 * t], tc1 = tcen[3 * t + 1], tc2 = tcen[3 * t + 2];
   for (int i = lane; i < 4 * NH; i += 32) acc[i] = 0.0;
   const int l0 = off[b], l1 = off[b + 1];
-  for (int lb = l0; lb < l1; lb += 32) {
-    const int l = lb + lane;
+  for (int lb = l0; lb < l1; lb += 16) {
+    const int l = lb + slot;
     const bool valid = l < l1;
     const double* src = multipole;
-    double cph = 1.0, sph = 0.0, cth = 1.0, sth = 0.0, rinv = 1.0;
+    double cph = 1.0, sph = 0.0, cth = 1.0, sth = 0.0, r = 1.0, rinv = 1.0;
     if (valid) {
       const int s = src_of[l];
       src = multipole + (int64_t)4 * NH * s;
       const double x = tc0 - scen[3 * s], y = tc1 - scen[3 * s + 1], z = tc2 - scen[3 * s + 2];
       const double x2y2 = x * x + y * y;
-      const double r = sqrt(x2y2 + z * z);
+      r = sqrt(x2y2 + z * z);
       if (x2y2 > 0) {
         const double rho = sqrt(x2y2);
         cph = x / rho;
@@ -1375,76 +1378,76 @@ __global__ void __launch_bounds__(32) k_m2l_lane_lh(const int* __restrict__ tgt_
         cth = z < 0 ? -1.0 : 1.0;
       }
       rinv = 1 / r;
-      if (p_used) p_used[l] = P;
+      if (p_used && set == 0) p_used[l] = P;
     }
     const V fcph = (V)cph, fsph = (V)sph, fcth = (V)cth, fsth = (V)sth;
-    // forward: both sets of every degree, rotated, scaled (t^-n and t^(1-n))
-    double sc = 1.0;  // t^-n
+    // forward: the lane's set of every degree, scaled (t^-n, t^(1-n)) and rotated
+    double sc = set ? r : 1.0;
 #pragma unroll 1
     for (int n = 0; n <= P; ++n) {
       if (n > 0) sc *= rinv;
-      const double sc1 = sc / rinv;  // t^(1-n)
-      V X0r[PMAX + 1], X0i[PMAX + 1], X1r[PMAX + 1], X1i[PMAX + 1];
+      V Xr[PMAX + 1], Xi[PMAX + 1];
       double er = 1.0, ei = 0.0;
       const int base = hi(n, 0);
 #pragma unroll
       for (int a = 0; a <= PMAX; ++a) {
-        X0r[a] = X0i[a] = X1r[a] = X1i[a] = V(0);
+        Xr[a] = Xi[a] = V(0);
         if (a > n || !valid) continue;
-        const double2 u = __ldg(reinterpret_cast<const double2*>(src) + 2 * (base + a));
-        const double2 v = __ldg(reinterpret_cast<const double2*>(src) + 2 * (base + a) + 1);
-        X0r[a] = (V)((u.x * er - u.y * ei) * sc);
-        X0i[a] = (V)((u.x * ei + u.y * er) * sc);
-        X1r[a] = (V)((v.x * er - v.y * ei) * sc1);
-        X1i[a] = (V)((v.x * ei + v.y * er) * sc1);
+        const double2 u = __ldg(reinterpret_cast<const double2*>(src) + 2 * (base + a) + set);
+        Xr[a] = (V)((u.x * er - u.y * ei) * sc);
+        Xi[a] = (V)((u.x * ei + u.y * er) * sc);
         const double tt = er;
         er = er * cph - ei * sph;
         ei = tt * sph + ei * cph;
       }
       V Yr[PMAX + 1], Yi[PMAX + 1];
-      rot_y<PMAX, false, V>(n, X0r, X0i, fcth, fsth, Yr, Yi);
+      rot_y<PMAX, false, V>(n, Xr, Xi, fcth, fsth, Yr, Yi);
 #pragma unroll
       for (int m = 0; m <= PMAX; ++m) {
         if (m > n) break;
-        MSl(Ms, base + m, 0, lane) = Yr[m];
-        MSl(Ms, base + m, 1, lane) = Yi[m];
-      }
-      rot_y<PMAX, false, V>(n, X1r, X1i, fcth, fsth, Yr, Yi);
-#pragma unroll
-      for (int m = 0; m <= PMAX; ++m) {
-        if (m > n) break;
-        MSl(Ms, base + m, 2, lane) = Yr[m];
-        MSl(Ms, base + m, 3, lane) = Yi[m];
+        Ms[(2 * (base + m)) * 32 + lane] = Yr[m];
+        Ms[(2 * (base + m) + 1) * 32 + lane] = Yi[m];
       }
     }
     __syncwarp();
-    // back: per degree the coaxial translation of set 0 (degree n) and of set 1 one degree
-    // ahead, the Lamb-Helmholtz coupling, both sets rotated back, scaled and staged
-    V C1r[PMAX + 1], C1i[PMAX + 1];  // set 1 of degree n before the coupling
-    coax_lh<PMAX, V>(0, P, Ms, 2, lane, C1r, C1i);
+    // back: the chi lane carries chi(n) (Cr, Ci) and translates chi(n + 1); the phi lane
+    // translates phi(n) and reads chi(n) from its chi lane
+    V Cr[PMAX + 1], Ci[PMAX + 1];
+    coax_lh<PMAX, V>(0, 0, P, Ms, lane, Cr, Ci);
     double tn1 = rinv;  // t^-(n+1)
 #pragma unroll 1
     for (int n = 0; n <= P; ++n) {
       if (n > 0) tn1 *= rinv;
-      const double tn2 = tn1 * rinv;
-      V N1r[PMAX + 1], N1i[PMAX + 1];  // set 1 of degree n + 1 before the coupling
-      if (n < P) {
-        coax_lh<PMAX, V>(n + 1, P, Ms, 2, lane, N1r, N1i);
+      const int nd = n + set;  // degree the lane translates
+      V Nr[PMAX + 1], Ni[PMAX + 1];
+      if (nd <= P) {
+        coax_lh<PMAX, V>(nd, n + 1, P, Ms, lane, Nr, Ni);
       } else {
 #pragma unroll
-        for (int m = 0; m <= PMAX; ++m) N1r[m] = N1i[m] = V(0);
+        for (int m = 0; m <= PMAX; ++m) Nr[m] = Ni[m] = V(0);
       }
       V Xr[PMAX + 1], Xi[PMAX + 1], Yr[PMAX + 1], Yi[PMAX + 1];
-      // set 0: phi(n, m) - i (m / n) chi(n, m)
-      coax_lh<PMAX, V>(n, P, Ms, 0, lane, Xr, Xi);
-      if (n > 0) {
-        const V inv_n = V(1) / (V)n;
+      const V inv_n = n > 0 ? V(1) / (V)n : V(0);
+      const V inv_n1 = V(1) / (V)(n + 1);
+#pragma unroll
+      for (int m = 0; m <= PMAX; ++m) {
+        Xr[m] = Xi[m] = V(0);
+        if (m > n) continue;
+        const V pr = __shfl_xor_sync(kAll, Cr[m], 16), pi = __shfl_xor_sync(kAll, Ci[m], 16);
+        if (set == 0) {  // phi(n, m) - i (m / n) chi(n, m)
+          const V a = (V)m * inv_n;
+          Xr[m] = Nr[m] - a * pi;
+          Xi[m] = Ni[m] + a * pr;
+        } else {  // chi(n, m) - chi(n + 1, m) / (n + 1)
+          Xr[m] = Cr[m] - inv_n1 * Nr[m];
+          Xi[m] = Ci[m] - inv_n1 * Ni[m];
+        }
+      }
+      if (set) {  // chi(n + 1) is the next step's chi(n)
 #pragma unroll
         for (int m = 0; m <= PMAX; ++m) {
-          if (m > n) break;
-          const V a = (V)m * inv_n;
-          Xr[m] -= a * C1i[m];
-          Xi[m] += a * C1r[m];
+          Cr[m] = Nr[m];
+          Ci[m] = Ni[m];
         }
       }
       rot_y<PMAX, true, V>(n, Xr, Xi, fcth, fsth, Yr, Yi);
@@ -1454,52 +1457,24 @@ __global__ void __launch_bounds__(32) k_m2l_lane_lh(const int* __restrict__ tgt_
         if (m > n) break;
         const V vr = Yr[m] * er + Yi[m] * ei;  // times e^{-i m phi}
         const V vi = Yi[m] * er - Yr[m] * ei;
-        stage[(4 * m) * 33 + lane] = valid ? vr : V(0);
-        stage[(4 * m + 1) * 33 + lane] = valid ? vi : V(0);
+        stage[(4 * m + 2 * set) * 17 + slot] = valid ? vr : V(0);
+        stage[(4 * m + 2 * set + 1) * 17 + slot] = valid ? vi : V(0);
         const V tt = er;
         er = er * fcph - ei * fsph;
         ei = tt * fsph + ei * fcph;
       }
-      // set 1: chi(n, m) - chi(n + 1, m) / (n + 1)
-      const V inv_n1 = V(1) / (V)(n + 1);
-#pragma unroll
-      for (int m = 0; m <= PMAX; ++m) {
-        Xr[m] = C1r[m] - inv_n1 * N1r[m];
-        Xi[m] = C1i[m] - inv_n1 * N1i[m];
-        if (m > n) Xr[m] = Xi[m] = V(0);
-      }
-      rot_y<PMAX, true, V>(n, Xr, Xi, fcth, fsth, Yr, Yi);
-      er = 1;
-      ei = 0;
-#pragma unroll
-      for (int m = 0; m <= PMAX; ++m) {
-        if (m > n) break;
-        const V vr = Yr[m] * er + Yi[m] * ei;
-        const V vi = Yi[m] * er - Yr[m] * ei;
-        stage[(4 * m + 2) * 33 + lane] = valid ? vr : V(0);
-        stage[(4 * m + 3) * 33 + lane] = valid ? vi : V(0);
-        const V tt = er;
-        er = er * fcph - ei * fsph;
-        ei = tt * fsph + ei * fcph;
-      }
-      tsc[lane] = tn1;
-      tsc[32 + lane] = tn2;
+      tsc[lane] = set ? tn1 * rinv : tn1;
       __syncwarp();
-      // 4 (n + 1) staged rows: more than the warp's 32 lanes from degree 8; each value times
-      // its lane's power of t in FP64 (set 0: t^-(n+1), set 1: t^-(n+2))
+      // 4 (n + 1) staged rows (order m, set, re/im), each value times its pair's power of t
+      // in FP64 (set 0: t^-(n+1), set 1: t^-(n+2))
       for (int row = lane; row < 4 * (n + 1); row += 32) {
-        const double* sc = tsc + ((row & 2) ? 32 : 0);
+        const double* ts = tsc + ((row & 2) ? 16 : 0);
         double v = 0.0;
-#pragma unroll 8
-        for (int k = 0; k < 32; ++k) v += (double)stage[row * 33 + k] * sc[k];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v += (double)stage[row * 17 + k] * ts[k];
         acc[4 * hi(n, 0) + row] += v;
       }
       __syncwarp();
-#pragma unroll
-      for (int m = 0; m <= PMAX; ++m) {
-        C1r[m] = N1r[m];
-        C1i[m] = N1i[m];
-      }
     }
     __syncwarp();
   }

@@ -217,3 +217,46 @@ def test_vjp_adjoint_workload_shape_finite_differences(ctx):
             fd = (lossq(buf, pp) - lossq(buf, pm)) / (2 * h)
             devs.append(abs(dy[i, k] - fd) / np.abs(dy).max())
     assert max(devs) <= 1e-5, max(devs)
+
+
+def test_vjp_gap_to_the_discrete_gradient(ctx):
+    # fmm_vjp is the continuous adjoint (a second FMM with the cotangents as strengths); the
+    # gradient ReverseDiff takes through the reference is the discrete one, the derivative of
+    # the FMM's own output.  Measured here against central differences of the FMM loss itself
+    # (FP64, same options; the loss is linear in the strengths, so those differences are exact
+    # up to rounding).  The exact gradient dL/dq_i = sum_t w_t / (4 pi r_ti) is the direct
+    # potential of sources of strength w.  The gap between the two FMM gradients is real (well
+    # above rounding) and no larger than the truncation error of the adjoint solve itself.
+    n = 3000
+    buf = bodies(n, L.FMM_POINT_SOURCE, 91)
+    rng = np.random.default_rng(92)
+    w = rng.standard_normal(n)
+    d_out = np.zeros((n, 16))
+    d_out[:, 3] = w
+    opt = fm.make_options(expansion_order=4, leaf_size_source=10, multipole_acceptance=0.6, scalar_potential=True)
+    _, dstr, _, _, _ = fm.vjp_buffers(buf, L.FMM_POINT_SOURCE, opt, d_out, None, ctx)
+    wbuf = buf.copy()
+    wbuf[:, 4] = w
+    exact = direct_out(ctx, wbuf, L.FMM_POINT_SOURCE)[:, 3]
+    sc = np.abs(exact).max()
+    adj_err = np.abs(dstr - exact).max() / sc
+    assert 1e-7 < adj_err < 1e-2, adj_err  # a visible truncation error at p = 4
+
+    def loss_fmm(b):
+        o, _ = fm.solve_buffers(b, L.FMM_POINT_SOURCE, opt, None, ctx)
+        return float(np.dot(w, o[:, 3]))
+
+    gaps, disc_err = [], []
+    for i in rng.choice(n, 12, replace=False):
+        hq = 1e-3 * max(abs(buf[i, 4]), 1e-3)
+        bp, bm = buf.copy(), buf.copy()
+        bp[i, 4] += hq
+        bm[i, 4] -= hq
+        disc = (loss_fmm(bp) - loss_fmm(bm)) / (2 * hq)
+        gaps.append(abs(dstr[i] - disc) / sc)
+        disc_err.append(abs(disc - exact[i]) / sc)
+    gap = max(gaps)
+    assert 1e-12 < gap <= 2 * adj_err, (gap, adj_err)
+    assert max(disc_err) <= 2 * adj_err, (max(disc_err), adj_err)
+    print(f"continuous adjoint vs discrete gradient: {gap:.2e}; adjoint vs exact (all bodies): {adj_err:.2e}; "
+          f"discrete vs exact (sampled): {max(disc_err):.2e}")
