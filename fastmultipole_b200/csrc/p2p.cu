@@ -327,7 +327,8 @@ __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y
 // test/vortex.jl:83-128).  acc[a] receives channel a of the two targets.  The gradient
 // du_j/dx_i = eps_jki G_k / r^3 - 3 d_i (G x d)_j / r^5 is summed as two parts, Q_ij =
 // sum d_i (G x d)_j / r^5 and E_k = sum G_k / r^3, combined once per batch (r^2 / r^5 =
-// 1 / r^3, so the six eps terms need three sums).  GUARD skips pairs with r^2 = 0
+// 1 / r^3, so the six eps terms need three sums; the trace of Q vanishes, so Q_zz is not
+// summed).  GUARD skips pairs with r^2 = 0
 // (coincident bodies); without it such a pair makes the sums non-finite.
 template <bool GUARD, bool GS, bool HS, int NA>
 __device__ __forceinline__ void packed_vortex_batch(const float4* __restrict__ B4, int j0, int nb, int SS,
@@ -377,7 +378,6 @@ __device__ __forceinline__ void packed_vortex_batch(const float4* __restrict__ B
       Q[5] = __ffma2_rn(py, cz, Q[5]);
       Q[6] = __ffma2_rn(pz, cx, Q[6]);
       Q[7] = __ffma2_rn(pz, cy, Q[7]);
-      Q[8] = __ffma2_rn(pz, cz, Q[8]);
       E[0] = __ffma2_rn(g0, den, E[0]);
       E[1] = __ffma2_rn(g1, den, E[1]);
       E[2] = __ffma2_rn(g2, den, E[2]);
@@ -389,6 +389,8 @@ __device__ __forceinline__ void packed_vortex_batch(const float4* __restrict__ B
     acc[2 % NA] = u[2];
   }
   if (HS) {
+    // the gradient is trace-free: d . (G x d) = 0 for every pair, so Q_zz = -(Q_xx + Q_yy)
+    Q[8] = neg2(__fadd2_rn(Q[0], Q[4]));
     const float2 m3 = make_float2(-3.f, -3.f);
     acc[(h + 0) % NA] = __fmul2_rn(m3, Q[0]);
     acc[(h + 1) % NA] = __ffma2_rn(m3, Q[1], E[2]);
@@ -479,11 +481,13 @@ __device__ __noinline__ void self_batch_f64_vortex(const double2* __restrict__ B
 // sums to the targets itself; otherwise one CTA per row, the warps splitting its sources.
 // W warps per CTA: kWarps, or kWideWarps for launches of few rows (one long row per CTA).
 // resident CTAs of the mixed instances: the registers the packed loop needs (the FP64
-// branch of the batch holding the target's own leaf is a call, and must not raise them)
+// branch of the batch holding the target's own leaf is a call, and must not raise them);
+// the FP64 vortex CTA path keeps 128 registers (4 CTAs per SM)
 template <class R, int KIND, bool HS, bool RW, int W>
 __host__ __device__ constexpr int p2p_min_blocks() {
   constexpr int regs = (KIND == FMM_POINT_VORTEX && HS) ? (RW ? 168 : 128) : (RW ? 72 : 64);
-  return sizeof(R) != 4 ? 1 : (65536 / (regs * W * 32) > 0 ? 65536 / (regs * W * 32) : 1);
+  if (sizeof(R) != 4) return (KIND == FMM_POINT_VORTEX && HS && !RW && W == kWarps) ? 4 : 1;
+  return 65536 / (regs * W * 32) > 0 ? 65536 / (regs * W * 32) : 1;
 }
 
 template <class R, int KIND, bool PS, bool GS, bool HS, bool RW, int W = kWarps>
@@ -516,10 +520,45 @@ __global__ void __launch_bounds__(W * 32, p2p_min_blocks<R, KIND, HS, RW, W>()) 
   const int4 ck = chunked ? chunks[blockIdx.x] : make_int4(0, 0, 0, 0);
   const int row = RW ? blockIdx.x * W + w : (chunked ? ck.x : (int)blockIdx.x);
   if (RW && row >= n_rows) return;  // whole warps: no block barrier on the RW path
-  constexpr int LS = RW ? 1 : W;  // stride of this warp's source leaves along the row
   const int t = tgt_list[row];
   const int l0 = chunked ? ck.y : off[row], l1 = chunked ? ck.z : off[row + 1];
   const int ts = t_start[t], tc = t_count[t];
+  // this warp's share of the row.  Vortex particles (CTA path): an equal contiguous range of
+  // the row's source bodies (leaves in row order, split inside a leaf where a range ends), so
+  // the warps reach the block's reduction together whatever the leaf sizes.  Point sources
+  // (CTA path): every W-th leaf (an even split measured no faster there, and its registers
+  // spill at the packed loop's 64).  One warp per row takes them all.
+  constexpr bool BAL = !RW && KIND == FMM_POINT_VORTEX;
+  constexpr int LS = (RW || BAL) ? 1 : W;  // stride of this warp's source leaves along the row
+  int lb0 = l0 + ((RW || BAL) ? 0 : w), poff0 = 0, rem0 = INT_MAX;
+  if (BAL) {
+    long long total = 0;
+    for (int i = l0 + lane; i < l1; i += 32) total += s_count[src_of[i]];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(kAll, total, o);
+    const int b_lo = (int)(total * w / W), b_hi = (int)(total * (w + 1) / W);
+    rem0 = b_hi - b_lo;
+    int before = 0;  // bodies of the leaves ahead of the current 32
+    for (int i0 = l0; i0 < l1 && rem0 > 0; i0 += 32) {
+      const int i = i0 + lane;
+      const int c = i < l1 ? s_count[src_of[i]] : 0;
+      int incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(kAll, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const unsigned past = __ballot_sync(kAll, i < l1 && before + incl > b_lo);
+      if (past) {  // the range starts inside leaf i0 + f
+        const int f = __ffs(past) - 1;
+        const int ex = __shfl_sync(kAll, incl - c, f);
+        lb0 = i0 + f;
+        poff0 = b_lo - before - ex;
+        break;
+      }
+      before += __shfl_sync(kAll, incl, 31);
+    }
+  }
   const double ox = MIXED ? t_center[3 * t] : 0.0;
   const double oy = MIXED ? t_center[3 * t + 1] : 0.0;
   const double oz = MIXED ? t_center[3 * t + 2] : 0.0;
@@ -553,9 +592,10 @@ __global__ void __launch_bounds__(W * 32, p2p_min_blocks<R, KIND, HS, RW, W>()) 
       for (int a = 0; a < 9; ++a) Qs[k][a] = R(0);
       Es[k][0] = Es[k][1] = Es[k][2] = R(0);
     }
-    int lb = l0 + (RW ? 0 : w), poff = 0;  // next source leaf of this warp, bodies of it already taken
-    while (lb < l1) {
-      // candidate leaves lb + W * lane; take the longest prefix that fits the batch
+    // next source leaf of this warp, bodies of it already taken, bodies of the range still to take
+    int lb = lb0, poff = poff0, rem = rem0;
+    while (lb < l1 && rem > 0) {
+      // candidate leaves lb + LS * lane; take the longest prefix that fits the batch and the range
       const int l = lb + LS * lane;
       int cnt = 0, sb = 0, sl = -1;
       if (l < l1) {
@@ -574,17 +614,19 @@ __global__ void __launch_bounds__(W * 32, p2p_min_blocks<R, KIND, HS, RW, W>()) 
         if (lane >= o) incl += v;
       }
       const int excl = incl - cnt;
-      int nl = __popc(__ballot_sync(kAll, l < l1 && incl <= NB));
+      const int lim = min(NB, rem);
+      int nl = __popc(__ballot_sync(kAll, l < l1 && incl <= lim));
       int nb;
-      if (nl == 0) {  // the first leaf alone overflows the batch: take NB bodies of it
+      if (nl == 0) {  // the first leaf alone overflows the batch or ends the range: lim bodies of it
         nl = 1;
-        nb = NB;
-        poff += NB;
+        nb = lim;
+        poff += lim;
       } else {
         nb = __shfl_sync(kAll, incl, nl - 1);
         lb += LS * nl;
         poff = 0;
       }
+      rem -= nb;
       // the batch holds the target branch's own bodies (coincident pairs certain)
       const bool self_batch = __any_sync(kAll, lane < nl && sl == t);
       // mixed path: that batch in FP64 (the solve's own near field; the influence estimate, which
