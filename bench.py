@@ -105,6 +105,11 @@ WORKLOADS = {
 # (tolerance, expansion order, multipole acceptance); MAC 0.5 converges like 0.5^(p+1) in the worst case
 MATCHED_CANDIDATES = [(1e-7, 12, 0.5), (3e-8, 12, 0.5), (1e-8, 12, 0.5), (1e-8, 16, 0.5)]
 
+# f32x2 operations the packed near-field loop issues per source and pair of targets, by
+# (kind, scalar potential, velocity gradient): point sources phi + grad 13 (grad alone 12),
+# vortex particles u + grad u 32
+NEAR_F32X2_OPS = {(1, True, False): 13, (1, False, False): 12, (3, False, True): 32}
+
 # DRAM bytes (read + write) of the solve's near-field launch, one ncu capture of the full-size
 # workload (dram__bytes_read.sum + dram__bytes_write.sum)
 NEAR_TRAFFIC = {"c2": 311889408 + 46925568, "c3": 5638054144 + 197501696}
@@ -389,6 +394,16 @@ def gpu_arm(args, w, rank, world, local_rank):
                 "peak_source": "measured on this GPU in this run (fmm_measure_fp32_peak: independent FMA chains; "
                                "MEASURED_PEAKS.json holds no CUDA-core figure)",
                 "peak_measured": meas, "peak_nominal": nominal_fp32, "frac_of_nominal": ach / nominal_fp32}
+        ops = NEAR_F32X2_OPS.get((w["kind"], w["ps"], w["hs"]))
+        if ops:
+            # the packed loop's own bound: its f32x2 operations per source and target pair at the
+            # measured f32x2 rate (4 flop per f32x2 FMA), independent of the flop convention above
+            bound_ms = st_mixed["n_p2p_pairs"] * ops / 2 / (meas["packed_f32x2"] * 1e12 / 4) * 1e3
+            roof["instruction_view"] = {
+                "f32x2_ops_per_source_and_two_targets": ops, "bound_ms": bound_ms,
+                "frac": bound_ms / stages["nearfield"],
+                "note": "operations counted in the packed loop (rsqrt runs on the XU pipe beside them); "
+                        "frac divides by the near field's event window, which also holds the concurrent far field"}
         if traffic:
             gbs = traffic / (stages["nearfield"] * 1e-3) / 1e9
             roof["hbm_view"] = {"achieved_gbs": gbs, "peak_gbs": pk.get("hbm_gbs"),

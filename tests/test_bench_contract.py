@@ -34,3 +34,11 @@ def test_accuracy_candidates_loosest_first():
     eps = [c[0] for c in bench.MATCHED_CANDIDATES]
     assert eps == sorted(eps, reverse=True)
     assert all(p <= 20 and 0 < mac < 1 for _, p, mac in bench.MATCHED_CANDIDATES)
+
+
+def test_every_near_field_workload_has_an_instruction_count():
+    # the roofline's instruction view needs the packed loop's operation count for each
+    # near-field-dominated workload the GPU arm times
+    for key in ("c1", "c2", "c3"):
+        w = bench.WORKLOADS[key]
+        assert (w["kind"], w["ps"], w["hs"]) in bench.NEAR_F32X2_OPS, key
