@@ -46,8 +46,11 @@ constexpr unsigned kAll = 0xffffffffu;
 // a sum run to the kernel's maximum order past the degree (its inputs are zero).
 constexpr int kLenTPad = kLenT + kLaneMaxP + 1;
 __constant__ double c_HBz[kLenTPad], c_HAz[kLenTPad], c_HBe[kLenTPad], c_HAe[kLenTPad];
-// single-precision copies for the mixed path, and k! for its scaled coaxial step
-__constant__ float c_HBzF[kLenTPad], c_HAzF[kLenTPad], c_HBeF[kLenTPad], c_HAeF[kLenTPad];
+// single-precision copies for the mixed path: column (n, nu) at float4 4 hi(n, nu), 16 floats
+// (entries past n zero), read four entries per constant load; and k! for its scaled coaxial step
+constexpr int kNCols = (kLaneMaxP + 1) * (kLaneMaxP + 2) / 2;
+constexpr int kColQ = 4;  // float4 per column (kLaneMaxP + 1 <= 16 entries)
+__constant__ float4 c_HBzQ[kNCols * kColQ], c_HAzQ[kNCols * kColQ], c_HBeQ[kNCols * kColQ], c_HAeQ[kNCols * kColQ];
 constexpr int kFact = 2 * kLaneMaxP + 2;
 __constant__ double c_fact[kFact];
 __constant__ float c_factF[kFact];
@@ -92,12 +95,22 @@ void ensure_lane_tables(cudaStream_t st) {
   FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAz, haz.data(), kLenTPad * 8, 0, cudaMemcpyHostToDevice, st));
   FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBe, hbe.data(), kLenTPad * 8, 0, cudaMemcpyHostToDevice, st));
   FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAe, hae.data(), kLenTPad * 8, 0, cudaMemcpyHostToDevice, st));
-  std::vector<float> fbz(hbz.begin(), hbz.end()), faz(haz.begin(), haz.end()), fbe(hbe.begin(), hbe.end()),
-      fae(hae.begin(), hae.end());
-  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBzF, fbz.data(), kLenTPad * 4, 0, cudaMemcpyHostToDevice, st));
-  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAzF, faz.data(), kLenTPad * 4, 0, cudaMemcpyHostToDevice, st));
-  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBeF, fbe.data(), kLenTPad * 4, 0, cudaMemcpyHostToDevice, st));
-  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAeF, fae.data(), kLenTPad * 4, 0, cudaMemcpyHostToDevice, st));
+  // the FP32 tables in padded columns
+  std::vector<float> fbz(kNCols * kColQ * 4, 0.f), faz(fbz), fbe(fbz), fae(fbz);
+  for (int n = 0; n <= kLaneMaxP; ++n)
+    for (int nu = 0; nu <= n; ++nu)
+      for (int a = 0; a <= n; ++a) {
+        const int src = lenT(n - 1) + nu * (n + 1) + a, dst = hi(n, nu) * kColQ * 4 + a;
+        fbz[dst] = (float)hbz[src];
+        faz[dst] = (float)haz[src];
+        fbe[dst] = (float)hbe[src];
+        fae[dst] = (float)hae[src];
+      }
+  const size_t qb = (size_t)kNCols * kColQ * sizeof(float4);
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBzQ, fbz.data(), qb, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAzQ, faz.data(), qb, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HBeQ, fbe.data(), qb, 0, cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_HAeQ, fae.data(), qb, 0, cudaMemcpyHostToDevice, st));
   std::vector<double> fact(kFact);
   std::vector<float> factf(kFact);
   fact[0] = 1.0;
@@ -121,65 +134,128 @@ void ensure_lane_tables(cudaStream_t st) {
 // schedule better than the skipped terms save).
 template <bool LOCAL, class V>
 __device__ __forceinline__ V tab_b(int i) {
-  if constexpr (sizeof(V) == 8)
-    return LOCAL ? c_HBe[i] : c_HBz[i];
-  else
-    return LOCAL ? c_HBeF[i] : c_HBzF[i];
+  return LOCAL ? c_HBe[i] : c_HBz[i];
 }
 template <bool LOCAL, class V>
 __device__ __forceinline__ V tab_a(int i) {
-  if constexpr (sizeof(V) == 8)
-    return LOCAL ? c_HAe[i] : c_HAz[i];
-  else
-    return LOCAL ? c_HAeF[i] : c_HAzF[i];
+  return LOCAL ? c_HAe[i] : c_HAz[i];
+}
+
+// FP32 rotate_y (the mixed path): rot_y below with the tables read as float4 quads of a
+// padded column, the same terms in the same order
+template <int PMAX, bool LOCAL>
+__device__ __forceinline__ void rot_y_q(int n, const float (&Xr)[PMAX + 1], const float (&Xi)[PMAX + 1], float cb,
+                                        float sb, float (&Yr)[PMAX + 1], float (&Yi)[PMAX + 1]) {
+  constexpr int NQ = PMAX / 4 + 1;  // quads covering entries 0..PMAX
+#pragma unroll
+  for (int m = 0; m <= PMAX; ++m) Yr[m] = Yi[m] = 0.f;
+  float c = 1.f, s = 0.f;  // cos, sin (nu beta) by the reference's recurrence
+#pragma unroll 1
+  for (int nu = 0; nu <= n; ++nu) {
+    if (nu > 0) {
+      const float cn = cb * c - sb * s;
+      const float sn = sb * c + cb * s;
+      c = cn;
+      s = sn;
+    }
+    const int q0 = hi(n, nu) * kColQ;
+    float Er = 0, Ei = 0, Or = 0, Oi = 0, h0 = 0;
+#pragma unroll
+    for (int aq = 0; aq < NQ; ++aq) {
+      const float4 h4 = LOCAL ? c_HBeQ[q0 + aq] : c_HBzQ[q0 + aq];
+      const float hh[4] = {h4.x, h4.y, h4.z, h4.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int a = 4 * aq + j;
+        if (a > PMAX) break;
+        if (a == 0) {
+          h0 = hh[0];
+        } else if (a & 1) {
+          Or += hh[j] * Xr[a];
+          Oi += hh[j] * Xi[a];
+        } else {
+          Er += hh[j] * Xr[a];
+          Ei += hh[j] * Xi[a];
+        }
+      }
+    }
+    const float Zr = h0 * Xr[0], Zi = h0 * Xi[0];
+    const float sg = ((n + nu) & 1) ? -1.f : 1.f;
+    const float S1r = Er - Or, S1i = Ei - Oi;
+    const float S3r = Er + Or, S3i = Ei + Oi;
+    const float S2r = Zr + S3r, S2i = -(Zi + S3i);
+    const float S4r = Zr + S1r, S4i = -(Zi + S1i);
+    const float A1r = S1r + sg * S2r, A1i = S1i + sg * S2i;
+    const float A3r = S3r + sg * S4r, A3i = S3i + sg * S4i;
+    const float ss = LOCAL ? -s : s;
+    const float Pr = c * A1r - ss * A1i, Pi = c * A1i + ss * A1r;
+    const float Qr = c * A3r + ss * A3i, Qi = c * A3i - ss * A3r;
+    const float Rpr = Pr + Qr, Rpi = Pi + Qi, Rmr = Pr - Qr, Rmi = Pi - Qi;
+#pragma unroll
+    for (int mq = 0; mq < NQ; ++mq) {
+      const float4 h4 = LOCAL ? c_HAeQ[q0 + mq] : c_HAzQ[q0 + mq];
+      const float hh[4] = {h4.x, h4.y, h4.z, h4.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int m = 4 * mq + j;
+        if (m > PMAX) break;
+        Yr[m] += hh[j] * ((m & 1) ? Rmr : Rpr);
+        Yi[m] += hh[j] * ((m & 1) ? Rmi : Rpi);
+      }
+    }
+  }
 }
 
 template <int PMAX, bool LOCAL, class V = double>
 __device__ __forceinline__ void rot_y(int n, const V (&Xr)[PMAX + 1], const V (&Xi)[PMAX + 1], V cb, V sb,
                                       V (&Yr)[PMAX + 1], V (&Yi)[PMAX + 1]) {
-  const int t0 = lenT(n - 1), w = n + 1;
+  if constexpr (sizeof(V) == 4) {
+    rot_y_q<PMAX, LOCAL>(n, Xr, Xi, cb, sb, Yr, Yi);
+  } else {
+    const int t0 = lenT(n - 1), w = n + 1;
 #pragma unroll
-  for (int m = 0; m <= PMAX; ++m) Yr[m] = Yi[m] = V(0);
-  V c = V(1), s = V(0);  // cos, sin (nu beta) by the reference's recurrence
+    for (int m = 0; m <= PMAX; ++m) Yr[m] = Yi[m] = V(0);
+    V c = V(1), s = V(0);  // cos, sin (nu beta) by the reference's recurrence
 #pragma unroll 1
-  for (int nu = 0; nu <= n; ++nu) {
-    if (nu > 0) {
-      const V cn = cb * c - sb * s;
-      const V sn = sb * c + cb * s;
-      c = cn;
-      s = sn;
-    }
-    const int col = t0 + nu * w;
-    V Er = 0, Ei = 0, Or = 0, Oi = 0;
-#pragma unroll
-    for (int a = 1; a <= PMAX; ++a) {
-      const V h = tab_b<LOCAL, V>(col + a);
-      if (a & 1) {
-        Or += h * Xr[a];
-        Oi += h * Xi[a];
-      } else {
-        Er += h * Xr[a];
-        Ei += h * Xi[a];
+    for (int nu = 0; nu <= n; ++nu) {
+      if (nu > 0) {
+        const V cn = cb * c - sb * s;
+        const V sn = sb * c + cb * s;
+        c = cn;
+        s = sn;
       }
-    }
-    const V h0 = tab_b<LOCAL, V>(col);
-    const V Zr = h0 * Xr[0], Zi = h0 * Xi[0];
-    const V sg = ((n + nu) & 1) ? V(-1) : V(1);
-    const V S1r = Er - Or, S1i = Ei - Oi;
-    const V S3r = Er + Or, S3i = Ei + Oi;
-    const V S2r = Zr + S3r, S2i = -(Zi + S3i);
-    const V S4r = Zr + S1r, S4i = -(Zi + S1i);
-    const V A1r = S1r + sg * S2r, A1i = S1i + sg * S2i;
-    const V A3r = S3r + sg * S4r, A3i = S3i + sg * S4i;
-    const V ss = LOCAL ? -s : s;
-    const V Pr = c * A1r - ss * A1i, Pi = c * A1i + ss * A1r;
-    const V Qr = c * A3r + ss * A3i, Qi = c * A3i - ss * A3r;
-    const V Rpr = Pr + Qr, Rpi = Pi + Qi, Rmr = Pr - Qr, Rmi = Pi - Qi;
+      const int col = t0 + nu * w;
+      V Er = 0, Ei = 0, Or = 0, Oi = 0;
 #pragma unroll
-    for (int m = 0; m <= PMAX; ++m) {
-      const V h = tab_a<LOCAL, V>(col + m);
-      Yr[m] += h * ((m & 1) ? Rmr : Rpr);
-      Yi[m] += h * ((m & 1) ? Rmi : Rpi);
+      for (int a = 1; a <= PMAX; ++a) {
+        const V h = tab_b<LOCAL, V>(col + a);
+        if (a & 1) {
+          Or += h * Xr[a];
+          Oi += h * Xi[a];
+        } else {
+          Er += h * Xr[a];
+          Ei += h * Xi[a];
+        }
+      }
+      const V h0 = tab_b<LOCAL, V>(col);
+      const V Zr = h0 * Xr[0], Zi = h0 * Xi[0];
+      const V sg = ((n + nu) & 1) ? V(-1) : V(1);
+      const V S1r = Er - Or, S1i = Ei - Oi;
+      const V S3r = Er + Or, S3i = Ei + Oi;
+      const V S2r = Zr + S3r, S2i = -(Zi + S3i);
+      const V S4r = Zr + S1r, S4i = -(Zi + S1i);
+      const V A1r = S1r + sg * S2r, A1i = S1i + sg * S2i;
+      const V A3r = S3r + sg * S4r, A3i = S3i + sg * S4i;
+      const V ss = LOCAL ? -s : s;
+      const V Pr = c * A1r - ss * A1i, Pi = c * A1i + ss * A1r;
+      const V Qr = c * A3r + ss * A3i, Qi = c * A3i - ss * A3r;
+      const V Rpr = Pr + Qr, Rpi = Pi + Qi, Rmr = Pr - Qr, Rmi = Pi - Qi;
+#pragma unroll
+      for (int m = 0; m <= PMAX; ++m) {
+        const V h = tab_a<LOCAL, V>(col + m);
+        Yr[m] += h * ((m & 1) ? Rmr : Rpr);
+        Yi[m] += h * ((m & 1) ? Rmi : Rpi);
+      }
     }
   }
 }
