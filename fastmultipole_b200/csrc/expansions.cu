@@ -465,7 +465,10 @@ __global__ void __launch_bounds__(32 * kWarps) k_p2m_lane(const int* __restrict_
           Pr[m] = Hr[m];
           Pi[m] = Hi[m];
         }
-        // q_nm1: (n-1, m-1) [m = 0: -conj-mirror of (n-1, 1)], (n-1, m), (n-1, m+1)
+        // q_nm1: (n-1, m-1) [m = 0: -conj-mirror of (n-1, 1)], (n-1, m), (n-1, m+1); the
+        // reference's division by n as a product with 1/n (one division per degree, not per
+        // coefficient; within an ulp of the quotient)
+        const double inv_n = 1.0 / n;
 #pragma unroll
         for (int m = 0; m <= PMAX; ++m) {
           if (m > n) continue;
@@ -480,8 +483,8 @@ __global__ void __launch_bounds__(32 * kWarps) k_p2m_lane(const int* __restrict_
           const double q2 = m < n ? Pr[m] : 0.0, q3 = m < n ? Pi[m] : 0.0;
           const double q4 = (m + 1 <= PMAX && m + 1 < n) ? Pr[(m + 1) % (PMAX + 1)] : 0.0;
           const double q5 = (m + 1 <= PMAX && m + 1 < n) ? Pi[(m + 1) % (PMAX + 1)] : 0.0;
-          Hr[m] = (-(xr * q1 + xi * q0) - (er * q5 + ei * q4) - z * q2) / n;
-          Hi[m] = ((xr * q0 - xi * q1) + (er * q4 - ei * q5) - z * q3) / n;
+          Hr[m] = (-(xr * q1 + xi * q0) - (er * q5 + ei * q4) - z * q2) * inv_n;
+          Hi[m] = ((xr * q0 - xi * q1) + (er * q4 - ei * q5) - z * q3) * inv_n;
         }
       }
       // degree-n contributions of this lane's body
@@ -797,6 +800,14 @@ __device__ void l2p_coefficients(double* C, const double* __restrict__ L, int p,
     __syncwarp();
 }
 
+// 1/k for the body-wise recursions (k <= 2 kMaxP + 1): a product with 1/k in place of the
+// division by k in the hot loops (within an ulp of the quotient)
+__constant__ double c_rcp[42] = {
+    0.0, 1.0 / 1, 1.0 / 2, 1.0 / 3, 1.0 / 4, 1.0 / 5, 1.0 / 6, 1.0 / 7, 1.0 / 8, 1.0 / 9, 1.0 / 10, 1.0 / 11,
+    1.0 / 12, 1.0 / 13, 1.0 / 14, 1.0 / 15, 1.0 / 16, 1.0 / 17, 1.0 / 18, 1.0 / 19, 1.0 / 20, 1.0 / 21,
+    1.0 / 22, 1.0 / 23, 1.0 / 24, 1.0 / 25, 1.0 / 26, 1.0 / 27, 1.0 / 28, 1.0 / 29, 1.0 / 30, 1.0 / 31,
+    1.0 / 32, 1.0 / 33, 1.0 / 34, 1.0 / 35, 1.0 / 36, 1.0 / 37, 1.0 / 38, 1.0 / 39, 1.0 / 40, 1.0 / 41};
+
 // contract one body: regular harmonics by the reference's column recursion
 __device__ void l2p_body(const double* C, int p, double x, double y, double z, bool ps, bool gs, bool hs, double* out) {
   const int NH = (p + 1) * (p + 2) / 2;
@@ -819,7 +830,7 @@ __device__ void l2p_body(const double* C, int p, double x, double y, double z, b
       if (n == m) {
         R = rhom * pl;
       } else {
-        rhon /= -(n + m);
+        rhon *= -c_rcp[n + m];
         R = rhon * pl;
       }
       double Rr = R * er, Ri = R * ei;
@@ -837,7 +848,7 @@ __device__ void l2p_body(const double* C, int p, double x, double y, double z, b
       } else {
         p2 = p1;
         p1 = pl;
-        pl = (cx * (2 * n + 1) * p1 - (n + m) * p2) / (n - m + 1);
+        pl = (cx * (2 * n + 1) * p1 - (n + m) * p2) * c_rcp[n - m + 1];
         rhon *= r;
       }
     }
