@@ -11,6 +11,14 @@
 namespace fmmb {
 
 constexpr int kMaxP = 20;         // highest expansion order the kernels are instantiated for
+// 1/k! for k = 0..kMaxP, correctly rounded: the coaxial translations multiply by these in place
+// of dividing by k! (within an ulp of the quotient)
+#define FMM_INV_FACTORIALS \
+    1.0, 1.0, 0.5, 0.16666666666666666, 0.041666666666666664, 0.008333333333333333, 0.001388888888888889, \
+    0.0001984126984126984, 2.48015873015873e-05, 2.7557319223985893e-06, 2.755731922398589e-07, \
+    2.505210838544172e-08, 2.08767569878681e-09, 1.6059043836821613e-10, 1.1470745597729725e-11, \
+    7.647163731819816e-13, 4.779477332387385e-14, 2.8114572543455206e-15, 1.5619206968586225e-16, \
+    8.22063524662433e-18, 4.110317623312165e-19
 constexpr int kMaxDepth = 21;     // octree levels representable by a 63-bit octant path key
 constexpr double kOneOver4Pi = 1.0 / (4.0 * 3.141592653589793);
 constexpr double kPi = 3.141592653589793;

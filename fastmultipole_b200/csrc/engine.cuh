@@ -19,6 +19,8 @@
 namespace fmmb {
 namespace eng {
 
+__constant__ double c_ifact[kMaxP + 1] = {FMM_INV_FACTORIALS};
+
 constexpr unsigned kFull = 0xffffffffu;
 
 struct Tab {
@@ -358,10 +360,9 @@ __device__ __forceinline__ void m2m_z_all(const WS& w, double* dst, const double
     int i = lane + 32 * k;
     if (i >= NHP) continue;
     int n = L.n[k], m = L.m[k];
-    double v1r = 0, v1i = 0, v2r = 0, v2i = 0, f = 1.0, tp = 1.0;
-    int q = 1;
+    double v1r = 0, v1i = 0, v2r = 0, v2i = 0, tp = 1.0;
     for (int np = n; np >= m; --np) {
-      double c = tp / f;
+      double c = tp * c_ifact[n - np];  // (-t)^(n-n') / (n-n')!
       int iw = np * (np + 1) / 2 + m;
       v1r += c * src[iw];
       v1i += c * src[NH + iw];
@@ -370,8 +371,6 @@ __device__ __forceinline__ void m2m_z_all(const WS& w, double* dst, const double
         v2i += c * src[3 * NH + iw];
       }
       tp *= _t;
-      f *= q;
-      q += 1;
     }
     dst[i] = v1r;
     dst[NH + i] = v1i;
@@ -393,9 +392,9 @@ __device__ __forceinline__ void l2l_z_all(const WS& w, double* dst, const double
     int i = lane + 32 * k;
     if (i >= NHP) continue;
     int n = L.n[k], m = L.m[k];
-    double v1r = 0, v1i = 0, v2r = 0, v2i = 0, c = 1.0;
-    int q = 1;
+    double v1r = 0, v1i = 0, v2r = 0, v2i = 0, tp = 1.0;
     for (int np = n; np <= P; ++np) {
+      const double c = tp * c_ifact[np - n];  // (-t)^(n'-n) / (n'-n)!
       int iw = np * (np + 1) / 2 + m;
       v1r += c * src[iw];
       v1i += c * src[NH + iw];
@@ -403,8 +402,7 @@ __device__ __forceinline__ void l2l_z_all(const WS& w, double* dst, const double
         v2r += c * src[2 * NH + iw];
         v2i += c * src[3 * NH + iw];
       }
-      c *= _t / q;
-      q += 1;
+      tp *= _t;
     }
     dst[i] = v1r;
     dst[NH + i] = v1i;

@@ -55,6 +55,7 @@ constexpr int kFact = 2 * kLaneMaxP + 2;
 __constant__ double c_fact[kFact];
 __constant__ float c_factF[kFact];
 __constant__ double c_Mt[kNhMax], c_Lt[kNhMax];
+__constant__ double c_ifact[kMaxP + 1] = {FMM_INV_FACTORIALS};
 
 __host__ __device__ constexpr int hi(int n, int m) { return n * (n + 1) / 2 + m; }
 __host__ __device__ constexpr int lenT(int n) { return n < 0 ? 0 : (n + 1) * (n + 2) * (2 * n + 3) / 6; }
@@ -967,11 +968,10 @@ __global__ void __launch_bounds__(32) k_m2m_lane(int l0, int l1, const int* __re
 #pragma unroll
     for (int m = 0; m <= PMAX; ++m) Xr[m] = Xi[m] = 0.0;
     {
-      double f = 1.0, tp = 1.0;
-      int q = 1;
+      double tp = 1.0;
 #pragma unroll 1
       for (int np = n; np >= 0; --np) {
-        const double cc = tp / f;
+        const double cc = tp * c_ifact[n - np];  // (-t)^(n-n') / (n-n')!
         const int base = hi(np, 0);
 #pragma unroll
         for (int m = 0; m <= PMAX; ++m) {
@@ -980,8 +980,6 @@ __global__ void __launch_bounds__(32) k_m2m_lane(int l0, int l1, const int* __re
           Xi[m] += cc * MSr(Ms, base + m, 1, lane);
         }
         tp *= mt;
-        f *= q;
-        q += 1;
       }
     }
     rot_y<PMAX, false>(n, Xr, Xi, g.cth, g.sth, Yr, Yi);
@@ -1037,16 +1035,16 @@ __global__ void __launch_bounds__(32) k_l2l_lane(int c0, int c1, const int* __re
   }
 #pragma unroll 1
   for (int n = 0; n <= PMAX; ++n) {
-    // translate_local_z!: out(n, m) = sum_{n' = n..P} prod_{q=1}^{n'-n} (-t / q) L(n', m); the
+    // translate_local_z!: out(n, m) = sum_{n' = n..P} (-t)^(n'-n) / (n'-n)! L(n', m); the
     // factor depends on n' - n only: source degrees outer, orders inner
     double Xr[PMAX + 1], Xi[PMAX + 1], Yr[PMAX + 1], Yi[PMAX + 1];
 #pragma unroll
     for (int m = 0; m <= PMAX; ++m) Xr[m] = Xi[m] = 0.0;
     {
-      double cc = 1.0;
-      int q = 1;
+      double tp = 1.0;
 #pragma unroll 1
       for (int np = n; np <= PMAX; ++np) {
+        const double cc = tp * c_ifact[np - n];  // (-t)^(n'-n) / (n'-n)!
         const int base = hi(np, 0);
 #pragma unroll
         for (int m = 0; m <= PMAX; ++m) {
@@ -1054,8 +1052,7 @@ __global__ void __launch_bounds__(32) k_l2l_lane(int c0, int c1, const int* __re
           Xr[m] += cc * MSr(Ls, base + m, 0, lane);
           Xi[m] += cc * MSr(Ls, base + m, 1, lane);
         }
-        cc *= mt / q;
-        q += 1;
+        tp *= mt;
       }
     }
     rot_y<PMAX, true>(n, Xr, Xi, g.cth, g.sth, Yr, Yi);
