@@ -811,11 +811,25 @@ __constant__ double c_rcp[42] = {
 // contract one body: regular harmonics by the reference's column recursion
 __device__ void l2p_body(const double* C, int p, double x, double y, double z, bool ps, bool gs, bool hs, double* out) {
   const int NH = (p + 1) * (p + 2) / 2;
-  double r, th, ph;
-  sph(x, y, z, r, th, ph);
-  double sy = sin(th), cx = cos(th);
+  // cos and sin of the polar angle and e^{i (phi + pi/2)} of cartesian_to_spherical
+  // (src/rotate.jl:9-21) straight from the offsets, without forming the angles (the same
+  // values up to rounding; on the z axis exact 0 where the trigonometric route leaves ~1e-16)
+  const double x2y2 = x * x + y * y;
+  const double r2 = x2y2 + z * z;
+  const double r = (r2 == 0.0) ? r2 : sqrt(r2);
+  double cx = 1.0, sy = 0.0, iei_r = 0.0, iei_i = 1.0;
+  if (r > 0) {
+    if (x2y2 > 0) {
+      const double rho = sqrt(x2y2);
+      cx = z / r;
+      sy = rho / r;
+      iei_r = -y / rho;
+      iei_i = x / rho;
+    } else {
+      cx = z < 0 ? -1.0 : 1.0;
+    }
+  }
   double fact = 1.0, pn = 1.0, rhom = 1.0;
-  double iei_i = sin(ph + kPi / 2), iei_r = cos(ph + kPi / 2);
   double er = 1.0, ei = 0.0;
   double a[kCh];
   for (int c = 0; c < kCh; ++c) a[c] = 0.0;
