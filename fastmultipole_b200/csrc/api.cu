@@ -688,7 +688,8 @@ size_t tree_bytes(const DevTree& t) {
 size_t lists_bytes(const DevLists& l) {
   return (l.m2l_t.cap + l.m2l_s.cap + l.dir_t.cap + l.dir_s.cap + l.m2l_tgt.cap + l.m2l_off.cap + l.dir_tgt.cap +
           l.dir_off.cap) *
-         4;
+             4 +
+         (l.p2p_chunks.cap + l.p2p_rowtab.cap) * sizeof(int4) + l.p2p_part.cap * 8;
 }
 
 template <class T>
@@ -705,7 +706,7 @@ void release_tree(DevTree& t) {
 
 void release_lists(DevLists& l) {
   rel(l.m2l_t); rel(l.m2l_s); rel(l.dir_t); rel(l.dir_s); rel(l.m2l_tgt); rel(l.m2l_off); rel(l.dir_tgt);
-  rel(l.dir_off);
+  rel(l.dir_off); rel(l.p2p_chunks); rel(l.p2p_rowtab); rel(l.p2p_part);
 }
 
 void release_scratch(Scratch& s) {
